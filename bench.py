@@ -1,0 +1,356 @@
+"""Benchmark: Fock builds/s on a 192x192 k-mesh, nb=8, layer-resolved V (1 GPU per rank).
+
+Workload: ``build_fock`` on a 192x192 mesh with nb=8 band channels, layer-
+resolved V_ab(q) = 2 pi tanh(|q| d_ab)/|q| (d_ab = 1 + |a-b|/2, V(0)=0), h from
+the seeded |R|<=3 Fourier model, P(k) = U diag(f) U^H with Haar U and
+f ~ U(0,1), complex128.  A step is STEP_BUILDS builds; before every build the
+L2 cache is flushed by writing a 256 MiB buffer (outside the timed interval)
+and each build is bracketed by CUDA events on the launching stream.
+
+``value``  = builds/s with inputs resident in HBM (sum of per-build device time).
+``e2e``    = builds/s through the public API with host buffers: H2D of P from
+             pinned memory, the build, D2H of Sigma and F, per step.
+``roofline`` = algorithmic bytes of one build / average build time against the
+             measured HBM copy bandwidth (MEASURED_PEAKS.json).
+``--impl reference`` times the CPU oracle (NumPy/SciPy restatement of the
+reference path, all host cores) on the same workload.
+Multi-GPU: independent replicas (the path has no exchange step); value = all
+ranks' builds / max-over-ranks device time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Fock builds/s & batched HF solves/s at |dE/E|<=1e-9, mixed vs plain FP64 (1 GPU)"
+UNIT = "builds/s"
+NK, NB = 192, 8
+STEP_BUILDS = 64
+WORKLOAD = "build_fock 192x192 mesh, nb=8, layer-resolved V, Haar density, complex128"
+
+
+def alg_bytes(nk1, nk2, nb, elem=16):
+    """Read P, h (complex) and VR (real), write Sigma and F: (4*16 + 8) nk^2 nb^2 B for complex128."""
+    return (4 * elem + elem // 2) * nk1 * nk2 * nb * nb
+
+
+def peaks():
+    try:
+        d = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """Samples nvidia-smi during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.p = None
+        self.gpu = gpu_index
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={gpu_index}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            out, _ = self.p.communicate(timeout=5)
+        except Exception:
+            self.p.kill()
+            out = ""
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def setup_dist(args):
+    import torch
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return ws, rank, local
+
+
+def make_inputs(seed, dtype=np.complex128):
+    from jax_hf_b200 import synthetic as S
+    prob, P = S.fock_build_192(seed)
+    return prob, P.astype(dtype)
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+    import jax_hf_b200 as G
+    from jax_hf_b200 import _lib
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    prob, P_np = make_inputs(1 + rank)
+    K = G.HartreeFockKernel(prob.weights, prob.hamiltonian, prob.coulomb_q, prob.T)
+    a = K.as_args()
+    P = torch.as_tensor(P_np, device=dev)
+    kw = dict(h=a["h"], VR=a["VR"], refP=a["refP"], HH=a["HH"], w2d=K.w2d, include_exchange=True,
+              include_hartree=False, exchange_hermitian_channel_packing=a["exchange_hermitian_channel_packing"],
+              contact_g=a["contact_g"], contact_Oi=a["contact_Oi"], contact_Oj=a["contact_Oj"])
+    Sg = torch.empty_like(P)
+    F = torch.empty_like(P)
+    H = torch.empty((1, 1, NB, NB), dtype=P.dtype, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def timed_builds(n, fn):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
+        for i in range(n):
+            flush.fill_(i & 0xFF)
+            ev[i][0].record(stream)
+            fn()
+            ev[i][1].record(stream)
+        return ev
+
+    def build():
+        G.build_fock(P, out=(Sg, H, F), **kw)
+
+    # warm-up
+    for _ in range(args.warmup):
+        timed_builds(args.builds_per_step, build)
+    torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clk = Clocks(local) if rank == 0 else None
+    t_wall = time.perf_counter()
+    evs = []
+    for _ in range(args.steps):
+        evs.append(timed_builds(args.builds_per_step, build))
+    torch.cuda.synchronize()
+    t_wall = time.perf_counter() - t_wall
+    clocks = clk.stop() if clk else None
+    if ws > 1:
+        torch.distributed.barrier()
+    per_build = [s.elapsed_time(e) for step in evs for (s, e) in step]   # ms
+    dev_ms = float(sum(per_build))
+    if ws > 1:
+        t = torch.tensor([dev_ms], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        dev_ms = float(t.item())
+    n_builds = args.steps * args.builds_per_step
+    value = ws * n_builds / (dev_ms / 1e3)
+    avg_us = 1e3 * float(np.mean(per_build))
+
+    # variants: complex64 storage and FP32 exchange FFT with complex128 storage
+    variants = {}
+    if not args.extras:
+        return _finish(args, ws, rank, value, dev_ms, avg_us, n_builds, t_wall, clocks, variants, None, None,
+                       P_np, prob)
+    P64 = P.to(torch.complex64)
+    K64 = G.HartreeFockKernel(prob.weights, prob.hamiltonian.astype(np.complex64), prob.coulomb_q, prob.T)
+    a64 = K64.as_args()
+    kw64 = dict(kw, h=a64["h"], VR=a64["VR"], refP=a64["refP"], HH=a64["HH"], w2d=K64.w2d,
+                contact_g=a64["contact_g"], contact_Oi=a64["contact_Oi"], contact_Oj=a64["contact_Oj"])
+    S64, F64 = torch.empty_like(P64), torch.empty_like(P64)
+    H64 = torch.empty((1, 1, NB, NB), dtype=P64.dtype, device=dev)
+    for name, fn, nbytes in (
+        ("c64", lambda: G.build_fock(P64, out=(S64, H64, F64), **kw64), alg_bytes(NK, NK, NB, 8)),
+        ("c128_fp32fft", lambda: G.build_fock(P, out=(Sg, H, F), fft_precision="fp32", **kw), alg_bytes(NK, NK, NB)),
+    ):
+        timed_builds(8, fn)
+        ev = timed_builds(STEP_BUILDS, fn)
+        torch.cuda.synchronize()
+        t = [s.elapsed_time(e) for (s, e) in ev]
+        us = 1e3 * float(np.mean(t))
+        variants[name] = {"builds_per_s": round(1e6 / us, 1), "us_per_build": round(us, 2),
+                          "achieved_gbs": round(nbytes / (us * 1e-6) / 1e9, 1)}
+
+    # e2e: public API with host buffers (H2D P from pinned memory, D2H Sigma and F)
+    hP = torch.from_numpy(P_np).pin_memory()
+    hS = torch.empty(P.shape, dtype=P.dtype).pin_memory()
+    hF = torch.empty(P.shape, dtype=P.dtype).pin_memory()
+    dP = torch.empty_like(P)
+
+    def e2e_step():
+        dP.copy_(hP, non_blocking=True)
+        G.build_fock(dP, out=(Sg, H, F), **kw)
+        hS.copy_(Sg, non_blocking=True)
+        hF.copy_(F, non_blocking=True)
+
+    for _ in range(3):
+        e2e_step()
+    torch.cuda.synchronize()
+    n_e2e = max(4, args.steps)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(n_e2e):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if ws > 1:
+        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_val = ws * n_e2e / (e2e_ms / 1e3)
+    nbytes_state = P.numel() * P.element_size()
+    return _finish(args, ws, rank, value, dev_ms, avg_us, n_builds, t_wall, clocks, variants, e2e_val,
+                   nbytes_state, P_np, prob)
+
+
+def _finish(args, ws, rank, value, dev_ms, avg_us, n_builds, t_wall, clocks, variants, e2e_val,
+            nbytes_state, P_np, prob):
+    if rank != 0:
+        return None
+    peak, peak_kind = peaks()
+    ab = alg_bytes(NK, NK, NB)
+    achieved = ab / (avg_us * 1e-6) / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "fock_build_192x192_nb8_c128_traffic.json"
+    if tf.exists():
+        try:
+            traffic = json.loads(tf.read_text()).get("dram_bytes_per_build")
+        except Exception:
+            traffic = None
+    line = {
+        "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(dev_ms / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD, "mesh": [NK, NK], "nb": NB,
+                   "l2": "flushed (256 MiB write) before every build", "parallelism": f"replicas x{ws}"},
+        "builds_per_step": args.builds_per_step,
+        "us_per_build": round(avg_us, 3),
+        "wall_s_timed": round(t_wall, 3),
+        "variants": variants,
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": traffic,
+                     "algorithmic_bytes_per_build": ab, "peak_source": peak_kind},
+        "e2e": None if e2e_val is None else {
+            "value": round(e2e_val, 1), "unit": UNIT, "h2d_bytes_per_step": nbytes_state,
+            "d2h_bytes_per_step": 2 * nbytes_state},
+        "gpu_launches": 3 * n_builds,
+        "clocks": clocks,
+    }
+    if args.cpu_baseline and ws == 1:
+        line["cpu_baseline"] = cpu_baseline(P_np, prob)
+    return line
+
+
+def oracle_build(prob, P, workers):
+    from oracle import hf_oracle as O
+    O.FFT_WORKERS = workers
+    Ko = O.Kernel(prob.weights, prob.hamiltonian, prob.coulomb_q, prob.T)
+    a = Ko.as_args()
+
+    def fn():
+        return O.build_fock(P, h=a["h"], VR=a["VR"], refP=a["refP"], HH=a["HH"], w2d=Ko.w2d,
+                            include_exchange=True, include_hartree=False,
+                            exchange_hermitian_channel_packing=a["exchange_hermitian_channel_packing"],
+                            contact_g=a["contact_g"], contact_Oi=a["contact_Oi"], contact_Oj=a["contact_Oj"])
+    return fn
+
+
+def cpu_baseline(P, prob, n=3):
+    cores = os.cpu_count() or 1
+    fn = oracle_build(prob, P, cores)
+    fn()
+    t = time.perf_counter()
+    for _ in range(n):
+        fn()
+    dt = (time.perf_counter() - t) / n
+    return {"value": round(1.0 / dt, 4), "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{n} oracle build_fock calls (NumPy/SciPy restatement, scipy.fft workers={cores}) "
+                      f"on the same 192x192 nb=8 input; {dt:.3f} s per build"}
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return None
+    prob, P = make_inputs(1)
+    cores = os.cpu_count() or 1
+    fn = oracle_build(prob, P, cores)
+    for _ in range(max(0, min(args.warmup, 1))):
+        fn()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        fn()
+    dt = time.perf_counter() - t
+    val = args.steps / dt
+    sample = (f"each step = 1 oracle build_fock (NumPy/SciPy restatement of jax_hf's path; JAX is not "
+              f"installed) on the 192x192 nb=8 complex128 input, scipy.fft workers={cores}")
+    return {
+        "impl": "reference", "metric": METRIC, "value": round(val, 4), "unit": UNIT, "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * dt / args.steps, 2),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+        "data": "synthetic (seeded)", "config": {"workload": WORKLOAD, "mesh": [NK, NK], "nb": NB},
+        "cpu_baseline": {"value": round(val, 4), "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": round(val, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--builds-per-step", type=int, default=STEP_BUILDS)
+    ap.add_argument("--no-extras", dest="extras", action="store_false",
+                    help="skip the c64 / FP32-FFT variants and the e2e leg (short runs for profiling)")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        ws = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        line = run_reference(args, ws, rank)
+    else:
+        ws, rank, local = setup_dist(args)
+        line = run_ours(args, ws, rank, local)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

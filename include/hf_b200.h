@@ -1,0 +1,139 @@
+/*
+ * hf_b200 — C ABI of the B200 (sm_100a) Fock-build / HF-objective library.
+ *
+ * Conventions
+ *  - Every entry point returns an int status (HF_OK == 0).  On failure
+ *    hf_last_error() returns a message for the calling thread.
+ *  - All array pointers are DEVICE pointers owned by the caller, in the
+ *    reference's row-major layouts:  P, h, refP, Sigma, F, Q: (nk1, nk2, nb, nb)
+ *    complex; p, eps: (nk1, nk2, nb) real; w2d: (nk1, nk2) real; VR:
+ *    (nk1, nk2, 1, 1) or (nk1, nk2, nb, nb), complex or real.  Complex values
+ *    are interleaved (re, im).  "dtype" selects the storage precision:
+ *    HF_C128 (complex128 / float64) or HF_C64 (complex64 / float32).
+ *  - `stream` is a cudaStream_t (NULL = legacy default stream).  No entry point
+ *    synchronises the stream; results are ready when the stream reaches them.
+ *  - Scratch memory is caller-provided ("workspace"); query its size first.
+ *    No entry point allocates device memory.
+ */
+#ifndef HF_B200_H
+#define HF_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes --------------------------------------------------------- */
+#define HF_OK 0
+#define HF_ERR_INVALID 1     /* bad argument or shape (the reference raises ValueError) */
+#define HF_ERR_UNSUPPORTED 2 /* size outside what this build implements           */
+#define HF_ERR_CUDA 3        /* a CUDA call or kernel launch failed               */
+#define HF_ERR_WORKSPACE 4   /* workspace missing or too small                    */
+#define HF_ERR_NONFINITE 5   /* non-finite value detected                         */
+#define HF_ERR_MAXITER 6     /* iteration cap reached (solver did not converge)   */
+#define HF_ERR_ABORTED 7     /* host abort flag was set                           */
+
+/* ---- storage precision ---------------------------------------------------- */
+#define HF_C128 0
+#define HF_C64 1
+
+/* ---- Fock-build flags ----------------------------------------------------- */
+#define HF_FOCK_EXCHANGE (1u << 0)  /* include_exchange                                */
+#define HF_FOCK_HARTREE (1u << 1)   /* include_hartree                                 */
+#define HF_FOCK_PACKING (1u << 2)   /* exchange_hermitian_channel_packing (scalar VR)  */
+#define HF_FOCK_VR_SCALAR (1u << 3) /* VR has shape (nk1, nk2, 1, 1)                   */
+#define HF_FOCK_VR_REAL (1u << 4)   /* VR is stored as a real array                    */
+#define HF_FOCK_FFT_FP32 (1u << 5)  /* complex128 storage, exchange FFT in FP32        */
+#define HF_FOCK_HAS_REFP (1u << 6)  /* refP is non-zero and must be subtracted         */
+
+const char* hf_last_error(void);
+const char* hf_status_string(int status);
+int hf_version(void);
+
+/* ---- Fock build ------------------------------------------------------------
+ * Replaces jax_hf.fock.build_fock (fock.py:18-97) -> utils.selfenergy_fft
+ * (utils.py:66-173) for block_specs=None and project_fn=None.
+ *   Sigma = -IFFT2(FFT2(P - refP) * VR) [+ contact sigma]     (all nb^2 channels, or
+ *           the upper triangle + conjugate when HF_FOCK_PACKING)
+ *   H     = diag(HH @ n), n_a = sum_k w_k Re(P - refP)_aa      (written as nb x nb; may be NULL)
+ *   F     = herm(h + Sigma + H)
+ * Contact terms (fock.py:77-92) are applied when n_contact > 0.
+ * HH, w2d, contact_g are real at the storage precision; contact_Oi/Oj complex (t, nb, nb).
+ * The exchange FFT runs on device in three passes (row FFT, column FFT x VR x
+ * column IFFT, row IFFT + fused epilogue) through `workspace`.
+ */
+int hf_fock_workspace_size(int dtype, unsigned flags, int nk1, int nk2, int nb, size_t* bytes);
+
+int hf_fock_build(void* stream, int dtype, unsigned flags, int nk1, int nk2, int nb,
+                  const void* P, const void* h, const void* VR, const void* refP,
+                  const void* HH, const void* w2d, int n_contact, const void* contact_g,
+                  const void* contact_Oi, const void* contact_Oj, void* Sigma, void* H, void* F,
+                  void* workspace, size_t workspace_bytes);
+
+/* ---- Objective reductions (compensated, FP64 accumulation) -----------------
+ * hf_energy replaces fock.hf_energy (fock.py:100-111):
+ *   E = sum_k w_k Re Tr[(h + (Sigma + H)/2) P]
+ * H_mode: 0 = no H, 1 = H is one nb x nb matrix for all k, 2 = H per k.
+ * hf_occupation_entropy replaces fock.occupation_entropy (fock.py:114-118);
+ * hf_free_energy replaces fock.free_energy (fock.py:121-129) with E read from
+ * device memory.  Scalar outputs are float64 device pointers.
+ */
+int hf_reduce_workspace_size(int nk1, int nk2, int nb, size_t* bytes);
+int hf_energy(void* stream, int dtype, int nk1, int nk2, int nb, const void* P, const void* h,
+              const void* Sigma, const void* H, int H_mode, const void* w2d, double* E_out,
+              void* workspace, size_t workspace_bytes);
+int hf_occupation_entropy(void* stream, int dtype, int nk1, int nk2, int nb, const void* p,
+                          const void* w_norm, double* S_out, void* workspace,
+                          size_t workspace_bytes);
+int hf_free_energy(void* stream, int dtype, int nk1, int nk2, int nb, const double* E,
+                   const void* p, const void* w_norm, double T, double* Omega_out,
+                   void* workspace, size_t workspace_bytes);
+
+/* ---- Chemical potential ------------------------------------------------------
+ * method 0: pure bisection            utils._find_mu_bisection (utils.py:353-382)
+ * method 1: Newton with bracket       utils._find_mu_newton    (utils.py:385-442)
+ * method 2: Newton-bracket from mu0   solver._solve_mu         (solver.py:62-101)
+ * maxiter <= 0 picks the reference default for the method and dtype.
+ * weights: method 0/1 take raw weights and n_electrons; method 2 takes the
+ * normalised weights and n_target_norm (as the solver does).  mu0 (device,
+ * float64) is read by method 2 only.  mu_out is a float64 device scalar.
+ */
+int hf_find_mu(void* stream, int dtype, int method, int nk1, int nk2, int nb, const void* eps,
+               const void* weights, double n_electrons, double T, int maxiter, const double* mu0,
+               double* mu_out);
+
+/* ---- Per-k small matrices (one warp per k-point) ------------------------------
+ * batch = number of nb x nb matrices (nk1*nk2 for mesh arrays).
+ * hf_density_from_Qp:   P = herm(Q diag(p) Q^H)            solver.py:42-44 (+ _herm)
+ * hf_fock_orbital:      Ft = Q^H F Q                        solver.py:47-49
+ * hf_eigh:              A = V diag(w) V^H, w ascending       jnp.linalg.eigh (LAPACK heevd)
+ * hf_cayley_retract:    U = (I + tau d/2)^-1 (I - tau d/2)   solver.py:122-138 (tau on host)
+ * hf_cayley_spectral:   (V, lam) = eigh(herm(i d))           solver.py:161-166
+ * hf_cayley_unitary:    U = V diag(c(tau, lam)) V^H          solver.py:169-182
+ * hf_diag_UFU:          diag(U^H Ft U) from V, Ft_eig, lam   solver.py:185-197
+ * hf_qr_retract:        U = QR(I - tau G), phase-fixed       solver.py:108-119
+ * Real outputs (w, lam, p, diag) are at the storage precision.
+ */
+int hf_density_from_Qp(void* stream, int dtype, int batch, int nb, const void* Q, const void* p,
+                       void* P);
+int hf_fock_orbital(void* stream, int dtype, int batch, int nb, const void* Q, const void* F,
+                    void* Ft);
+int hf_eigh(void* stream, int dtype, int batch, int nb, const void* A, void* w, void* V);
+int hf_cayley_retract(void* stream, int dtype, int batch, int nb, const void* d, double tau,
+                      void* U);
+int hf_cayley_spectral(void* stream, int dtype, int batch, int nb, const void* d, void* V,
+                       void* lam);
+int hf_cayley_unitary(void* stream, int dtype, int batch, int nb, const void* V, const void* lam,
+                      double tau, void* U);
+int hf_diag_UFU(void* stream, int dtype, int batch, int nb, const void* V, const void* Ft_eig,
+                const void* lam, double tau, void* diag);
+int hf_qr_retract(void* stream, int dtype, int batch, int nb, const void* G, double tau,
+                  void* U);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HF_B200_H */

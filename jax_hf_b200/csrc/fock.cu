@@ -1,0 +1,546 @@
+// Fock build on B200: exchange convolution by batched 2D FFT + fused epilogue.
+//
+// Replaces jax_hf.fock.build_fock (fock.py:18-97) with
+// utils.selfenergy_fft (utils.py:66-173) inside it:
+//   Sigma_ab(k) = -IFFT2( FFT2(P - refP)_ab * VR_ab )(k)   (channels independent)
+//   F = herm(h + Sigma + H)
+//
+// Three passes over a slot-grouped spectrum in the caller's workspace
+// (layout [group][k1][k2][slot], complex at the FFT precision):
+//   K1 row pass     : load (P - refP) row k1 for one slot group, FFT along k2.
+//   K2 column pass  : FFT along k1, multiply by -VR/(nk1 nk2), IFFT along k1.
+//   K3 row pass     : IFFT along k2, then the epilogue (contact sigma, Hartree
+//                     diagonal, herm with the transposed channel, h-add) writes
+//                     Sigma and F once.
+// A slot group is a set of band-pair channels closed under transposition
+// (2x2 channel tiles paired with their transposes), so the hermitisation of
+// F needs no extra pass, and each 2x2 tile keeps 32-byte sectors whole.
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "common.cuh"
+#include "fft_engine.cuh"
+
+namespace hf {
+
+constexpr int kMaxNb = 32;
+constexpr int kMaxSlotTable = 1280;
+constexpr int kThreads = 256;
+
+struct FockParams {
+  int nk1, nk2, nb, nb2, LS, ngroups;
+  unsigned flags;
+  int n_contact;
+  double scale;  // -1 / (nk1 nk2)
+  FftPlan1D row, col;
+  const void* P;
+  const void* h;
+  const void* VR;
+  const void* refP;
+  const void* w2d;
+  const void* HH;
+  const void* cg;
+  const void* cOi;
+  const void* cOj;
+  void* Sigma;
+  void* F;
+  void* Hout;
+  void* scratch;
+  double2* rho_part;  // [nk1][ngroups*LS]
+  double2* sigc;      // [nb*nb] contact sigma
+  double* hdiag;      // [nb] Hartree diagonal
+  int16_t chan[kMaxSlotTable];
+  int16_t partner[kMaxSlotTable];
+};
+
+// ------------------------------------------------------------ planning -----
+struct SlotPlan {
+  int LS = 0, ngroups = 0;
+  std::vector<int16_t> chan, partner;
+};
+
+static FftPlan1D make_fft_plan(int n) {
+  FftPlan1D p{};
+  p.n = n;
+  int m = n, k = 0;
+  auto push = [&](int r) { p.radix[k++] = r; m /= r; };
+  while (m % 8 == 0 && k < kMaxStages) push(8);
+  while (m % 4 == 0 && k < kMaxStages) push(4);
+  while (m % 2 == 0 && k < kMaxStages) push(2);
+  while (m % 5 == 0 && k < kMaxStages) push(5);
+  while (m % 3 == 0 && k < kMaxStages) push(3);
+  for (int f = 7; m > 1 && k < kMaxStages; f += 2)
+    while (m % f == 0 && k < kMaxStages) push(f);
+  p.nstages = k;
+  return p;
+}
+
+// Units are transpose-closed channel sets built from 2x2 tiles; full mode pairs
+// tile (I,J) with (J,I); packing mode keeps the upper triangle only.
+static std::vector<std::vector<int>> make_units(int nb, bool packing) {
+  std::vector<std::vector<int>> units;
+  const int T = (nb + 1) / 2;
+  auto tile = [&](int I, int J, bool upper_only) {
+    std::vector<int> v;
+    for (int a = 2 * I; a < std::min(2 * I + 2, nb); ++a)
+      for (int b = 2 * J; b < std::min(2 * J + 2, nb); ++b)
+        if (!upper_only || a <= b) v.push_back(a * nb + b);
+    return v;
+  };
+  for (int I = 0; I < T; ++I)
+    for (int J = I; J < T; ++J) {
+      std::vector<int> u = tile(I, J, packing);
+      if (!packing && J > I) {
+        std::vector<int> t = tile(J, I, false);
+        u.insert(u.end(), t.begin(), t.end());
+      }
+      units.push_back(u);
+    }
+  return units;
+}
+
+static bool pack_units(const std::vector<std::vector<int>>& units, int LS,
+                       std::vector<std::vector<int>>& groups) {
+  groups.clear();
+  std::vector<int> order(units.size());
+  for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int x, int y) { return units[x].size() > units[y].size(); });
+  for (int ui : order) {
+    const auto& u = units[ui];
+    if ((int)u.size() > LS) return false;
+    bool placed = false;
+    for (auto& g : groups)
+      if ((int)(g.size() + u.size()) <= LS) {
+        g.insert(g.end(), u.begin(), u.end());
+        placed = true;
+        break;
+      }
+    if (!placed) groups.push_back(u);
+  }
+  return true;
+}
+
+template <typename FT>
+static size_t fock_smem_bytes(int n, int LS) {
+  return (size_t)(2 * n * LS + n) * sizeof(cpx_t<FT>);
+}
+
+static int plan_slots(int nb, bool packing, int nmax, size_t celem, SlotPlan& out) {
+  auto units = make_units(nb, packing);
+  int maxu = 0, total = 0;
+  for (auto& u : units) { maxu = std::max<int>(maxu, (int)u.size()); total += (int)u.size(); }
+  const size_t kTwoPerSm = 113 * 1024, kOnePerSm = 227 * 1024;
+  int best = -1, best_pad = 1 << 30, best_fit2 = 0;
+  std::vector<std::vector<int>> groups, best_groups;
+  for (int LS = maxu; LS <= 32; ++LS) {
+    if (!pack_units(units, LS, groups)) continue;
+    size_t smem = (size_t)(2 * nmax * LS + nmax) * celem;
+    if (smem > kOnePerSm) continue;
+    int pad = (int)groups.size() * LS - total;
+    int fit2 = smem <= kTwoPerSm ? 1 : 0;
+    bool better = false;
+    if (best < 0) better = true;
+    else if (fit2 != best_fit2) better = fit2 > best_fit2;
+    else if (pad != best_pad) better = pad < best_pad;
+    else better = std::abs(LS - 16) < std::abs(best - 16);
+    if (better) { best = LS; best_pad = pad; best_fit2 = fit2; best_groups = groups; }
+  }
+  if (best < 0) return HF_ERR_UNSUPPORTED;
+  out.LS = best;
+  out.ngroups = (int)best_groups.size();
+  out.chan.assign(out.LS * out.ngroups, -1);
+  out.partner.assign(out.LS * out.ngroups, -1);
+  for (int g = 0; g < out.ngroups; ++g) {
+    const auto& grp = best_groups[g];
+    for (size_t s = 0; s < grp.size(); ++s) out.chan[g * out.LS + s] = (int16_t)grp[s];
+    for (size_t s = 0; s < grp.size(); ++s) {
+      int a = grp[s] / nb, b = grp[s] % nb;
+      int want = b * nb + a;
+      int16_t pidx = (int16_t)s;
+      if (!packing)
+        for (size_t t = 0; t < grp.size(); ++t)
+          if (grp[t] == want) pidx = (int16_t)t;
+      out.partner[g * out.LS + s] = pidx;
+    }
+  }
+  if ((int)out.chan.size() > kMaxSlotTable) return HF_ERR_UNSUPPORTED;
+  return HF_OK;
+}
+
+// ------------------------------------------------------------- kernels -----
+template <typename ST, typename FT>
+__global__ void __launch_bounds__(kThreads) k_fock_row_fwd(const __grid_constant__ FockParams p) {
+  using SC = cpx_t<ST>;
+  using FC = cpx_t<FT>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int N = p.nk2, LS = p.LS;
+  FC* tw = reinterpret_cast<FC*>(smem_raw);
+  FC* b0 = tw + N;
+  FC* b1 = b0 + N * LS;
+  const int k1 = blockIdx.x, g = blockIdx.y;
+  build_twiddles<FT>(tw, N);
+  const SC* P = static_cast<const SC*>(p.P);
+  const SC* refP = static_cast<const SC*>(p.refP);
+  const bool has_ref = (p.flags & HF_FOCK_HAS_REFP) != 0;
+  const size_t row0 = (size_t)k1 * N;
+  for (int it = threadIdx.x; it < N * LS; it += blockDim.x) {
+    const int i = it / LS, s = it - i * LS;
+    const int c = p.chan[g * LS + s];
+    FC v = mk<FC>(0.0, 0.0);
+    if (c >= 0) {
+      const size_t idx = (row0 + i) * p.nb2 + c;
+      SC x = P[idx];
+      if (has_ref) x = csub(x, refP[idx]);
+      v = cvt<FC>(x);
+    }
+    b0[it] = v;
+  }
+  __syncthreads();
+  FC* res = fft_lines<false>(p.row, b0, b1, tw, LS);
+  FC* out = static_cast<FC*>(p.scratch) + (((size_t)g * p.nk1 + k1) * N) * LS;
+  for (int it = threadIdx.x; it < N * LS; it += blockDim.x) out[it] = res[it];
+}
+
+// Weighted density partial sums for Hartree / contact terms: rho_part[k1][slot]
+// = sum_{k2} w(k1,k2) (P - refP)(k1,k2)[chan(slot)], accumulated in float64.
+template <typename ST>
+__global__ void __launch_bounds__(kThreads) k_fock_rho_part(const __grid_constant__ FockParams p) {
+  using SC = cpx_t<ST>;
+  __shared__ double2 red[kThreads];
+  const int N = p.nk2, LS = p.LS;
+  const int k1 = blockIdx.x, g = blockIdx.y;
+  const int parts = kThreads / LS;
+  const int s = threadIdx.x % LS, part = threadIdx.x / LS;
+  const SC* P = static_cast<const SC*>(p.P);
+  const SC* refP = static_cast<const SC*>(p.refP);
+  const ST* w = static_cast<const ST*>(p.w2d);
+  const bool has_ref = (p.flags & HF_FOCK_HAS_REFP) != 0;
+  double2 acc = make_double2(0.0, 0.0);
+  const int c = p.chan[g * LS + s];
+  if (part < parts && c >= 0) {
+    for (int i = part; i < N; i += parts) {
+      const size_t kk = (size_t)k1 * N + i;
+      SC x = P[kk * p.nb2 + c];
+      if (has_ref) x = csub(x, refP[kk * p.nb2 + c]);
+      const double wk = (double)w[kk];
+      acc.x += wk * (double)x.x;
+      acc.y += wk * (double)x.y;
+    }
+  }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  if (threadIdx.x < LS) {
+    double2 t = make_double2(0.0, 0.0);
+    for (int q = 0; q < parts; ++q) t = cadd(t, red[q * LS + threadIdx.x]);
+    p.rho_part[(size_t)k1 * (p.ngroups * LS) + g * LS + threadIdx.x] = t;
+  }
+}
+
+template <typename ST, typename FT>
+__global__ void __launch_bounds__(kThreads) k_fock_col(const __grid_constant__ FockParams p) {
+  using SC = cpx_t<ST>;
+  using FC = cpx_t<FT>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int N = p.nk1, LS = p.LS;
+  FC* tw = reinterpret_cast<FC*>(smem_raw);
+  FC* b0 = tw + N;
+  FC* b1 = b0 + N * LS;
+  const int k2 = blockIdx.x, g = blockIdx.y;
+  build_twiddles<FT>(tw, N);
+  FC* sc = static_cast<FC*>(p.scratch) + ((size_t)g * p.nk1 * p.nk2 + k2) * LS;
+  const size_t rstride = (size_t)p.nk2 * LS;
+  for (int it = threadIdx.x; it < N * LS; it += blockDim.x) {
+    const int i = it / LS, s = it - i * LS;
+    b0[it] = sc[i * rstride + s];
+  }
+  __syncthreads();
+  FC* x = fft_lines<false>(p.col, b0, b1, tw, LS);
+  const bool vr_scalar = (p.flags & HF_FOCK_VR_SCALAR) != 0;
+  const bool vr_real = (p.flags & HF_FOCK_VR_REAL) != 0;
+  for (int it = threadIdx.x; it < N * LS; it += blockDim.x) {
+    const int q1 = it / LS, s = it - q1 * LS;
+    const int c = p.chan[g * LS + s];
+    if (c < 0) { x[it] = mk<FC>(0.0, 0.0); continue; }
+    const size_t q = (size_t)q1 * p.nk2 + k2;
+    const size_t vi = vr_scalar ? q : q * p.nb2 + c;
+    FC v = x[it];
+    if (vr_real) {
+      const FT r = (FT)((double)static_cast<const ST*>(p.VR)[vi] * p.scale);
+      v = cscale(v, r);
+    } else {
+      SC z = static_cast<const SC*>(p.VR)[vi];
+      FC zz = mk<FC>((double)z.x * p.scale, (double)z.y * p.scale);
+      v = cmul(v, zz);
+    }
+    x[it] = v;
+  }
+  __syncthreads();
+  FC* other = (x == b0) ? b1 : b0;
+  FC* y = fft_lines<true>(p.col, x, other, tw, LS);
+  for (int it = threadIdx.x; it < N * LS; it += blockDim.x) {
+    const int i = it / LS, s = it - i * LS;
+    sc[i * rstride + s] = y[it];
+  }
+}
+
+// Reduces rho partials and forms the k-independent terms (fock.py:66-92).
+template <typename ST>
+__global__ void k_fock_consts(const __grid_constant__ FockParams p) {
+  using SC = cpx_t<ST>;
+  __shared__ double2 rho[kMaxNb * kMaxNb];
+  const int nb = p.nb, nb2 = p.nb2, LS = p.LS, ns = p.ngroups * LS;
+  const bool packing = (p.flags & HF_FOCK_PACKING) != 0;
+  for (int c = threadIdx.x; c < nb2; c += blockDim.x) rho[c] = make_double2(0.0, 0.0);
+  __syncthreads();
+  for (int s = threadIdx.x; s < ns; s += blockDim.x) {
+    const int c = p.chan[s];
+    if (c < 0) continue;
+    double2 t = make_double2(0.0, 0.0);
+    for (int k1 = 0; k1 < p.nk1; ++k1) t = cadd(t, p.rho_part[(size_t)k1 * ns + s]);
+    rho[c] = t;
+    const int a = c / nb, b = c % nb;
+    if (packing && a != b) rho[b * nb + a] = conj(t);
+  }
+  __syncthreads();
+  // Hartree diagonal: HH @ n, n_a = Re rho_aa (fock.py:66-74)
+  if (p.flags & HF_FOCK_HARTREE) {
+    const ST* HH = static_cast<const ST*>(p.HH);
+    for (int a = threadIdx.x; a < nb; a += blockDim.x) {
+      double acc = 0.0;
+      for (int b = 0; b < nb; ++b) acc += (double)HH[a * nb + b] * rho[b * nb + b].x;
+      p.hdiag[a] = (double)(ST)acc;
+    }
+  } else {
+    for (int a = threadIdx.x; a < nb; a += blockDim.x) p.hdiag[a] = 0.0;
+  }
+  // contact: sum_t g_t [Oi_t tr(Oj_t rho) - Oi_t rho Oj_t] (fock.py:77-92)
+  const SC* Oi = static_cast<const SC*>(p.cOi);
+  const SC* Oj = static_cast<const SC*>(p.cOj);
+  const ST* gg = static_cast<const ST*>(p.cg);
+  for (int c = threadIdx.x; c < nb2; c += blockDim.x) {
+    const int i = c / nb, l = c % nb;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int t = 0; t < p.n_contact; ++t) {
+      const SC* oi = Oi + (size_t)t * nb2;
+      const SC* oj = Oj + (size_t)t * nb2;
+      double2 tr = make_double2(0.0, 0.0);
+      for (int a = 0; a < nb; ++a)
+        for (int b = 0; b < nb; ++b) tr = cadd(tr, cmul(cvt<double2>(oj[a * nb + b]), rho[b * nb + a]));
+      const double gt = (double)gg[t];
+      double2 hterm = cscale(cmul(cvt<double2>(oi[i * nb + l]), tr), gt);
+      double2 fterm = make_double2(0.0, 0.0);
+      for (int j = 0; j < nb; ++j) {
+        double2 oir = make_double2(0.0, 0.0);
+        for (int k = 0; k < nb; ++k) oir = cadd(oir, cmul(cvt<double2>(oi[i * nb + k]), rho[k * nb + j]));
+        fterm = cadd(fterm, cmul(oir, cvt<double2>(oj[j * nb + l])));
+      }
+      acc = cadd(acc, csub(hterm, cscale(fterm, gt)));
+    }
+    p.sigc[c] = acc;
+  }
+  __syncthreads();
+  if (p.Hout) {
+    SC* Ho = static_cast<SC*>(p.Hout);
+    for (int c = threadIdx.x; c < nb2; c += blockDim.x) {
+      const int a = c / nb, b = c % nb;
+      Ho[c] = mk<SC>(a == b ? p.hdiag[a] : 0.0, 0.0);
+    }
+  }
+}
+
+template <typename ST, typename FT>
+__global__ void __launch_bounds__(kThreads) k_fock_row_inv(const __grid_constant__ FockParams p) {
+  using SC = cpx_t<ST>;
+  using FC = cpx_t<FT>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int N = p.nk2, LS = p.LS, nb = p.nb;
+  FC* tw = reinterpret_cast<FC*>(smem_raw);
+  FC* b0 = tw + N;
+  FC* b1 = b0 + N * LS;
+  const int k1 = blockIdx.x, g = blockIdx.y;
+  const bool exch = (p.flags & HF_FOCK_EXCHANGE) != 0;
+  const bool packing = (p.flags & HF_FOCK_PACKING) != 0;
+  FC* res = b0;
+  if (exch) {
+    build_twiddles<FT>(tw, N);
+    const FC* sc = static_cast<const FC*>(p.scratch) + (((size_t)g * p.nk1 + k1) * N) * LS;
+    for (int it = threadIdx.x; it < N * LS; it += blockDim.x) b0[it] = sc[it];
+    __syncthreads();
+    res = fft_lines<true>(p.row, b0, b1, tw, LS);
+  } else {
+    for (int it = threadIdx.x; it < N * LS; it += blockDim.x) b0[it] = mk<FC>(0.0, 0.0);
+    __syncthreads();
+  }
+  const SC* h = static_cast<const SC*>(p.h);
+  SC* Sg = static_cast<SC*>(p.Sigma);
+  SC* F = static_cast<SC*>(p.F);
+  const bool consts = p.sigc != nullptr;
+  for (int it = threadIdx.x; it < N * LS; it += blockDim.x) {
+    const int i = it / LS, s = it - i * LS;
+    const int c = p.chan[g * LS + s];
+    if (c < 0) continue;
+    const int a = c / nb, b = c - (c / nb) * nb;
+    const size_t base = ((size_t)k1 * N + i) * p.nb2;
+    SC sab = cvt<SC>(res[it]);
+    SC sba;
+    if (packing) sba = (a == b) ? sab : conj(sab);
+    else sba = cvt<SC>(res[i * LS + p.partner[g * LS + s]]);
+    if (consts) {
+      sab = cadd(sab, cvt<SC>(p.sigc[a * nb + b]));
+      sba = cadd(sba, cvt<SC>(p.sigc[b * nb + a]));
+    }
+    const SC hab = h[base + a * nb + b];
+    const SC hba = h[base + b * nb + a];
+    SC f = mk<SC>(0.5 * ((double)hab.x + (double)hba.x) + 0.5 * ((double)sab.x + (double)sba.x),
+                  0.5 * ((double)hab.y - (double)hba.y) + 0.5 * ((double)sab.y - (double)sba.y));
+    if (consts && a == b) f.x += (ST)p.hdiag[a];
+    Sg[base + a * nb + b] = sab;
+    F[base + a * nb + b] = f;
+    if (packing && a != b) {
+      Sg[base + b * nb + a] = sba;
+      F[base + b * nb + a] = conj(f);
+    }
+  }
+}
+
+// ---------------------------------------------------------- host driver ----
+struct WsLayout {
+  size_t scratch = 0, rho = 0, sigc = 0, hdiag = 0, total = 0;
+};
+
+static WsLayout ws_layout(const SlotPlan& sp, int nk1, int nk2, int nb, size_t felem, bool exch) {
+  WsLayout w;
+  size_t off = 0;
+  w.scratch = off;
+  if (exch) off += align_up((size_t)sp.ngroups * sp.LS * nk1 * nk2 * felem, 256);
+  w.rho = off;
+  off += align_up((size_t)nk1 * sp.ngroups * sp.LS * sizeof(double2), 256);
+  w.sigc = off;
+  off += align_up((size_t)nb * nb * sizeof(double2), 256);
+  w.hdiag = off;
+  off += align_up((size_t)nb * sizeof(double), 256);
+  w.total = off;
+  return w;
+}
+
+static int validate(int dtype, unsigned flags, int nk1, int nk2, int nb) {
+  if (dtype != HF_C128 && dtype != HF_C64) return fail(HF_ERR_INVALID, "dtype must be HF_C128 or HF_C64");
+  if (nk1 < 1 || nk2 < 1 || nb < 1) return fail(HF_ERR_INVALID, "nk1, nk2, nb must be positive");
+  if (nb > kMaxNb) return fail(HF_ERR_UNSUPPORTED, "nb > 32 is not supported by this build");
+  if (!(flags & (HF_FOCK_EXCHANGE | HF_FOCK_HARTREE)))
+    return fail(HF_ERR_INVALID, "HartreeFockKernel must include at least one of Hartree or exchange.");
+  if ((flags & HF_FOCK_PACKING) && !(flags & HF_FOCK_VR_SCALAR))
+    return fail(HF_ERR_INVALID,
+                "hermitian_channel_packing requires a scalar interaction kernel with shape (..., 1, 1).");
+  if ((flags & HF_FOCK_FFT_FP32) && dtype != HF_C128)
+    return fail(HF_ERR_INVALID, "HF_FOCK_FFT_FP32 applies to complex128 storage only");
+  return HF_OK;
+}
+
+static size_t fft_elem(int dtype, unsigned flags) {
+  return (dtype == HF_C64 || (flags & HF_FOCK_FFT_FP32)) ? sizeof(float2) : sizeof(double2);
+}
+
+static int get_plan(int dtype, unsigned flags, int nk1, int nk2, int nb, SlotPlan& sp) {
+  const bool packing = (flags & HF_FOCK_PACKING) != 0;
+  int st = plan_slots(nb, packing, std::max(nk1, nk2), fft_elem(dtype, flags), sp);
+  if (st != HF_OK) return fail(st, "mesh too large for the shared-memory FFT (nk1, nk2 <= 768 in complex128)");
+  return HF_OK;
+}
+
+template <typename ST, typename FT>
+static int launch_fock(FockParams& p, cudaStream_t stream, bool need_consts) {
+  const bool exch = (p.flags & HF_FOCK_EXCHANGE) != 0;
+  const size_t sm_row = fock_smem_bytes<FT>(p.nk2, p.LS);
+  const size_t sm_col = fock_smem_bytes<FT>(p.nk1, p.LS);
+  HF_CUDA(cudaFuncSetAttribute(k_fock_row_fwd<ST, FT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_row));
+  HF_CUDA(cudaFuncSetAttribute(k_fock_col<ST, FT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_col));
+  HF_CUDA(cudaFuncSetAttribute(k_fock_row_inv<ST, FT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_row));
+  dim3 grow(p.nk1, p.ngroups), gcol(p.nk2, p.ngroups);
+  if (need_consts) {
+    k_fock_rho_part<ST><<<grow, kThreads, 0, stream>>>(p);
+    HF_LAUNCH_CHECK("k_fock_rho_part");
+    k_fock_consts<ST><<<1, 256, 0, stream>>>(p);
+    HF_LAUNCH_CHECK("k_fock_consts");
+  }
+  if (exch) {
+    k_fock_row_fwd<ST, FT><<<grow, kThreads, sm_row, stream>>>(p);
+    HF_LAUNCH_CHECK("k_fock_row_fwd");
+    k_fock_col<ST, FT><<<gcol, kThreads, sm_col, stream>>>(p);
+    HF_LAUNCH_CHECK("k_fock_col");
+  }
+  k_fock_row_inv<ST, FT><<<grow, kThreads, sm_row, stream>>>(p);
+  HF_LAUNCH_CHECK("k_fock_row_inv");
+  return HF_OK;
+}
+
+}  // namespace hf
+
+using namespace hf;
+
+extern "C" int hf_fock_workspace_size(int dtype, unsigned flags, int nk1, int nk2, int nb, size_t* bytes) {
+  if (!bytes) return fail(HF_ERR_INVALID, "bytes is NULL");
+  int st = validate(dtype, flags, nk1, nk2, nb);
+  if (st) return st;
+  SlotPlan sp;
+  if ((st = get_plan(dtype, flags, nk1, nk2, nb, sp))) return st;
+  *bytes = ws_layout(sp, nk1, nk2, nb, fft_elem(dtype, flags), (flags & HF_FOCK_EXCHANGE) != 0).total;
+  return HF_OK;
+}
+
+extern "C" int hf_fock_build(void* stream, int dtype, unsigned flags, int nk1, int nk2, int nb,
+                             const void* P, const void* h, const void* VR, const void* refP,
+                             const void* HH, const void* w2d, int n_contact, const void* contact_g,
+                             const void* contact_Oi, const void* contact_Oj, void* Sigma, void* H,
+                             void* F, void* workspace, size_t workspace_bytes) {
+  int st = validate(dtype, flags, nk1, nk2, nb);
+  if (st) return st;
+  const bool exch = (flags & HF_FOCK_EXCHANGE) != 0;
+  if (!P || !h || !Sigma || !F) return fail(HF_ERR_INVALID, "P, h, Sigma and F must be non-NULL");
+  if (exch && !VR) return fail(HF_ERR_INVALID, "VR must be non-NULL when exchange is included");
+  if ((flags & HF_FOCK_HAS_REFP) && !refP) return fail(HF_ERR_INVALID, "refP flagged but NULL");
+  if ((flags & HF_FOCK_HARTREE) && (!HH || !w2d)) return fail(HF_ERR_INVALID, "Hartree needs HH and w2d");
+  if (n_contact < 0) return fail(HF_ERR_INVALID, "n_contact must be >= 0");
+  if (n_contact > 0 && (!contact_g || !contact_Oi || !contact_Oj || !w2d))
+    return fail(HF_ERR_INVALID, "contact terms need g, O_i, O_j and w2d");
+  SlotPlan sp;
+  if ((st = get_plan(dtype, flags, nk1, nk2, nb, sp))) return st;
+  WsLayout wl = ws_layout(sp, nk1, nk2, nb, fft_elem(dtype, flags), exch);
+  if (!workspace || workspace_bytes < wl.total)
+    return fail(HF_ERR_WORKSPACE, "workspace too small: need " + std::to_string(wl.total) + " bytes");
+  if (reinterpret_cast<uintptr_t>(workspace) % 256 != 0)
+    return fail(HF_ERR_WORKSPACE, "workspace must be 256-byte aligned");
+
+  FockParams p;
+  memset(&p, 0, sizeof(p));
+  p.nk1 = nk1; p.nk2 = nk2; p.nb = nb; p.nb2 = nb * nb;
+  p.LS = sp.LS; p.ngroups = sp.ngroups;
+  p.flags = flags; p.n_contact = n_contact;
+  p.scale = -1.0 / ((double)nk1 * (double)nk2);
+  p.row = make_fft_plan(nk2);
+  p.col = make_fft_plan(nk1);
+  p.P = P; p.h = h; p.VR = VR; p.refP = refP; p.w2d = w2d; p.HH = HH;
+  p.cg = contact_g; p.cOi = contact_Oi; p.cOj = contact_Oj;
+  p.Sigma = Sigma; p.F = F; p.Hout = H;
+  char* ws = static_cast<char*>(workspace);
+  p.scratch = ws + wl.scratch;
+  const bool need_consts = (flags & HF_FOCK_HARTREE) || n_contact > 0;
+  if (need_consts) {
+    p.rho_part = reinterpret_cast<double2*>(ws + wl.rho);
+    p.sigc = reinterpret_cast<double2*>(ws + wl.sigc);
+    p.hdiag = reinterpret_cast<double*>(ws + wl.hdiag);
+  }
+  std::copy(sp.chan.begin(), sp.chan.end(), p.chan);
+  std::copy(sp.partner.begin(), sp.partner.end(), p.partner);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (H && !need_consts) {
+    const size_t hb = (size_t)nb * nb * (dtype == HF_C128 ? sizeof(double2) : sizeof(float2));
+    HF_CUDA(cudaMemsetAsync(H, 0, hb, s));
+  }
+  if (dtype == HF_C64) return launch_fock<float, float>(p, s, need_consts);
+  if (flags & HF_FOCK_FFT_FP32) return launch_fock<double, float>(p, s, need_consts);
+  return launch_fock<double, double>(p, s, need_consts);
+}

@@ -1,0 +1,228 @@
+// Chemical potential: mu such that sum_k w_k sum_j f(eps_kj - mu) = N.
+//
+// One thread-block cluster (up to 8 CTAs x 1024 threads) runs the whole root
+// find: every iteration each CTA reduces its slice, publishes the partial in
+// its shared memory, one cluster barrier, and every CTA then sums all partials
+// through distributed shared memory in rank order.  All CTAs therefore hold
+// bit-identical (mu, lo, hi) and take identical branches; no global-memory
+// round trip and no second launch per iteration.
+//
+// Methods (reference):
+//   0  _find_mu_bisection  utils.py:353-382 (maxiter 54 f64 / 30 f32)
+//   1  _find_mu_newton     utils.py:385-442 (maxiter 25 f64 / 15 f32)
+//   2  _solve_mu           solver.py:62-101 (maxiter 25, warm start mu0)
+// The iterations replay the reference update rules.  Bisection stops early
+// only at an exact fixed point of (lo, hi); the Newton variants stop once the
+// accepted Newton step is below 4 ulp of mu (the reference keeps iterating
+// there, moving mu by at most a few ulp).
+#include <cooperative_groups.h>
+
+#include "common.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace hf {
+
+constexpr int kMuThreads = 1024;
+constexpr int kMuMaxCluster = 8;
+
+struct MuArgs {
+  const void* eps;
+  const void* w;
+  int n, nb, method, maxiter;
+  double target, T;
+  const double* mu0;
+  double* out;
+};
+
+template <typename RT>
+__device__ __forceinline__ double load_eps(const MuArgs& a, int e) {
+  return (double)static_cast<const RT*>(a.eps)[e];
+}
+template <typename RT>
+__device__ __forceinline__ double load_w(const MuArgs& a, int e) {
+  return (double)static_cast<const RT*>(a.w)[e / a.nb];
+}
+
+// cluster-wide sum of (x, y); every thread of every CTA receives the total.
+__device__ __forceinline__ void cluster_sum2(cg::cluster_group& cl, double& x, double& y,
+                                             double (*slots)[2], double* wsm, int parity) {
+  x = warp_sum(x);
+  y = warp_sum(y);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (lane == 0) { wsm[2 * wid] = x; wsm[2 * wid + 1] = y; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double sx = 0.0, sy = 0.0;
+    for (int i = 0; i < nw; ++i) { sx += wsm[2 * i]; sy += wsm[2 * i + 1]; }
+    slots[parity][0] = sx;
+    slots[parity][1] = sy;
+  }
+  cl.sync();
+  double tx = 0.0, ty = 0.0;
+  const unsigned nbk = cl.num_blocks();
+  for (unsigned r = 0; r < nbk; ++r) {
+    double(*rs)[2] = cl.map_shared_rank(slots, r);
+    tx += rs[parity][0];
+    ty += rs[parity][1];
+  }
+  x = tx;
+  y = ty;
+}
+
+__device__ __forceinline__ void cluster_minmax(cg::cluster_group& cl, double& mn, double& mx,
+                                               double (*slots)[2], double* wsm) {
+  for (int off = 16; off > 0; off >>= 1) {
+    mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, off));
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (lane == 0) { wsm[2 * wid] = mn; wsm[2 * wid + 1] = mx; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = wsm[0], b = wsm[1];
+    for (int i = 1; i < nw; ++i) { a = fmin(a, wsm[2 * i]); b = fmax(b, wsm[2 * i + 1]); }
+    slots[2][0] = a;
+    slots[2][1] = b;
+  }
+  cl.sync();
+  double a = INFINITY, b = -INFINITY;
+  for (unsigned r = 0; r < cl.num_blocks(); ++r) {
+    double(*rs)[2] = cl.map_shared_rank(slots, r);
+    a = fmin(a, rs[2][0]);
+    b = fmax(b, rs[2][1]);
+  }
+  mn = a;
+  mx = b;
+}
+
+__device__ __forceinline__ double expit(double x) { return 1.0 / (1.0 + exp(-x)); }
+
+template <typename RT>
+__global__ void __launch_bounds__(kMuThreads) k_find_mu(const MuArgs a) {
+  cg::cluster_group cl = cg::this_cluster();
+  __shared__ double slots[3][2];
+  __shared__ double wsm[64];
+  const int gt = cl.block_rank() * blockDim.x + threadIdx.x;
+  const int gs = cl.num_blocks() * blockDim.x;
+
+  double mn = INFINITY, mx = -INFINITY;
+  for (int e = gt; e < a.n; e += gs) {
+    const double v = load_eps<RT>(a, e);
+    mn = fmin(mn, v);
+    mx = fmax(mx, v);
+  }
+  cluster_minmax(cl, mn, mx, slots, wsm);
+
+  int parity = 0;
+  double result;
+  if (a.method == 0) {
+    const double T = a.T;
+    const double span = mx - mn + 10.0 * fmax(T, 1e-6);
+    double lo = mn - span, hi = mx + span;
+    const double Td = T + 1e-12;
+    for (int it = 0; it < a.maxiter; ++it) {
+      const double mid = 0.5 * (lo + hi);
+      double cnt = 0.0, dummy = 0.0;
+      for (int e = gt; e < a.n; e += gs)
+        cnt += load_w<RT>(a, e) * expit(-(load_eps<RT>(a, e) - mid) / Td);
+      cluster_sum2(cl, cnt, dummy, slots, wsm, parity);
+      parity ^= 1;
+      const double nlo = (cnt > a.target) ? lo : mid;
+      const double nhi = (cnt > a.target) ? mid : hi;
+      if (nlo == lo && nhi == hi) break;  // exact fixed point
+      lo = nlo;
+      hi = nhi;
+    }
+    result = 0.5 * (lo + hi);
+  } else {
+    const double Tj = fmax(a.T, 1e-12);
+    double lo, hi, mu;
+    if (a.method == 1) {
+      const double span = mx - mn + 10.0 * fmax(Tj, 1e-6);
+      lo = mn - span;
+      hi = mx + span;
+      mu = 0.5 * (lo + hi);
+    } else {
+      lo = mn - 50.0 * Tj;
+      hi = mx + 50.0 * Tj;
+      const double m0 = a.mu0 ? a.mu0[0] : 0.0;
+      mu = fmin(fmax(m0, lo), hi);
+    }
+    for (int it = 0; it < a.maxiter; ++it) {
+      double N = 0.0, Z = 0.0;
+      for (int e = gt; e < a.n; e += gs) {
+        const double w = load_w<RT>(a, e);
+        const double p = expit((mu - load_eps<RT>(a, e)) / Tj);
+        N += w * p;
+        Z += w * (p * (1.0 - p)) / Tj;
+      }
+      cluster_sum2(cl, N, Z, slots, wsm, parity);
+      parity ^= 1;
+      const double g = N - a.target;
+      if (g < 0) lo = mu;
+      if (g > 0) hi = mu;
+      double mn2 = mu - g / fmax(Z, 1e-18);
+      const double mb = 0.5 * (lo + hi);
+      bool newton = true;
+      if (mn2 <= lo || mn2 >= hi) { mn2 = mb; newton = false; }
+      mn2 = fmin(fmax(mn2, lo), hi);
+      if (!isfinite(mn2)) { mn2 = mb; newton = false; }
+      const double step = fabs(mn2 - mu);
+      mu = mn2;
+      if (newton && step <= 4.0 * 2.220446049250313e-16 * fmax(1.0, fabs(mu))) break;
+    }
+    if (a.method == 1) {
+      double N = 0.0, dummy = 0.0;
+      for (int e = gt; e < a.n; e += gs)
+        N += load_w<RT>(a, e) * expit((mu - load_eps<RT>(a, e)) / Tj);
+      cluster_sum2(cl, N, dummy, slots, wsm, parity);
+      parity ^= 1;
+      if (fabs(N - a.target) > 1e-12) mu = 0.5 * (lo + hi);
+    }
+    result = mu;
+  }
+  if (cl.block_rank() == 0 && threadIdx.x == 0) a.out[0] = result;
+  cl.sync();  // keep every CTA's shared memory alive until all remote reads are done
+}
+
+}  // namespace hf
+
+using namespace hf;
+
+extern "C" int hf_find_mu(void* stream, int dtype, int method, int nk1, int nk2, int nb,
+                          const void* eps, const void* weights, double n_electrons, double T,
+                          int maxiter, const double* mu0, double* mu_out) {
+  if (dtype != HF_C128 && dtype != HF_C64) return fail(HF_ERR_INVALID, "bad dtype");
+  if (method < 0 || method > 2) return fail(HF_ERR_INVALID, "method must be 0, 1 or 2");
+  if (nk1 < 1 || nk2 < 1 || nb < 1) return fail(HF_ERR_INVALID, "bad shape");
+  if (!eps || !weights || !mu_out) return fail(HF_ERR_INVALID, "NULL argument");
+  const bool single = dtype == HF_C64;
+  if (maxiter <= 0) {
+    if (method == 0) maxiter = single ? 30 : 54;
+    else if (method == 1) maxiter = single ? 15 : 25;
+    else maxiter = 25;
+  }
+  MuArgs a;
+  a.eps = eps; a.w = weights;
+  a.n = nk1 * nk2 * nb; a.nb = nb; a.method = method; a.maxiter = maxiter;
+  a.target = n_electrons; a.T = T; a.mu0 = mu0; a.out = mu_out;
+  int csize = (a.n + 4 * kMuThreads - 1) / (4 * kMuThreads);
+  if (csize < 1) csize = 1;
+  if (csize > kMuMaxCluster) csize = kMuMaxCluster;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(csize, 1, 1);
+  cfg.blockDim = dim3(kMuThreads, 1, 1);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = static_cast<cudaStream_t>(stream);
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = csize;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (single) HF_CUDA(cudaLaunchKernelEx(&cfg, k_find_mu<float>, a));
+  else HF_CUDA(cudaLaunchKernelEx(&cfg, k_find_mu<double>, a));
+  return HF_OK;
+}
