@@ -132,6 +132,54 @@ int hf_diag_UFU(void* stream, int dtype, int batch, int nb, const void* V, const
 int hf_qr_retract(void* stream, int dtype, int batch, int nb, const void* G, double tau,
                   void* U);
 
+/* ---- Device-resident solvers ---------------------------------------------------
+ * The problem is a HartreeFockKernel's arrays (problem.py:201-217 as_args) in
+ * complex128 storage.  fock_flags carries HF_FOCK_EXCHANGE/HARTREE/PACKING/
+ * VR_SCALAR/VR_REAL/HAS_REFP exactly as for hf_fock_build.
+ */
+typedef struct hf_cg_problem {
+  int nk1, nk2, nb;
+  unsigned fock_flags;
+  double T, n_electrons, weight_sum;
+  const void* h;          /* (nk1, nk2, nb, nb) complex128                 */
+  const void* VR;         /* phase-shifted VR (complex128 or float64)       */
+  const void* refP;       /* may be NULL unless HF_FOCK_HAS_REFP            */
+  const void* HH;         /* (nb, nb) float64, may be NULL without Hartree  */
+  const void* w2d;        /* (nk1, nk2) float64 raw weights                 */
+  int n_contact;
+  const void* contact_g;  /* (t,) float64                                   */
+  const void* contact_Oi; /* (t, nb, nb) complex128                         */
+  const void* contact_Oj;
+} hf_cg_problem;
+
+/* SolverConfig fields (solver.py:240-286) plus the mixed-precision policy:
+ * fp32_exchange != 0 runs the exchange FFT in FP32 until the windowed energy
+ * change reaches fp32_switch_rel*|E| (or half of max_iter), then continues with
+ * FP64 builds (defect correction) to tol_E / tol_grad; the final builds are FP64.
+ * chunk = iterations queued between host checks of the device stop flag. */
+typedef struct hf_cg_config {
+  int max_iter;
+  double tol_E, tol_grad, denom_scale, max_step;
+  int cg_restart;
+  double bt_shrink;
+  int bt_max, mu_maxiter, plateau_window;
+  int fp32_exchange;
+  double fp32_switch_rel;
+  int chunk;
+} hf_cg_config;
+
+/* Direct-minimisation CG (solver.py:307-660, optimizer="cg"): replaces
+ * jax_hf.solve / solve_direct_minimization for project_fn=None, block_sizes=None.
+ * Inputs: P0 (nk1, nk2, nb, nb) complex128.  Outputs (device): Q, p, density,
+ * fock as in SolveResult; hist_E / hist_grad (max_iter float64, may be NULL);
+ * scalars_out (8 float64): mu, energy, n_iter, converged, last grad_norm,
+ * iteration of the FP32->FP64 switch (-1 if none), 0, 0.
+ * Synchronises `stream` once per chunk of iterations and at the end. */
+int hf_cg_workspace_size(const hf_cg_problem* problem, const hf_cg_config* config, size_t* bytes);
+int hf_cg_solve(void* stream, const hf_cg_problem* problem, const hf_cg_config* config, const void* P0,
+                void* Q, void* p, void* density, void* fock, double* hist_E, double* hist_grad,
+                double* scalars_out, void* workspace, size_t workspace_bytes);
+
 #ifdef __cplusplus
 }
 #endif

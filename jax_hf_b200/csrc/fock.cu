@@ -51,6 +51,7 @@ struct FockParams {
   double2* rho_part;  // [nk1][ngroups*LS]
   double2* sigc;      // [nb*nb] contact sigma
   double* hdiag;      // [nb] Hartree diagonal
+  const int* active;  // optional device flag: kernels return at once when *active == 0
   int16_t chan[kMaxSlotTable];
   int16_t partner[kMaxSlotTable];
 };
@@ -173,6 +174,7 @@ static int plan_slots(int nb, bool packing, int nmax, size_t celem, SlotPlan& ou
 // ------------------------------------------------------------- kernels -----
 template <typename ST, typename FT>
 __global__ void __launch_bounds__(kThreads) k_fock_row_fwd(const __grid_constant__ FockParams p) {
+  if (p.active && !*p.active) return;
   using SC = cpx_t<ST>;
   using FC = cpx_t<FT>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -208,6 +210,7 @@ __global__ void __launch_bounds__(kThreads) k_fock_row_fwd(const __grid_constant
 // = sum_{k2} w(k1,k2) (P - refP)(k1,k2)[chan(slot)], accumulated in float64.
 template <typename ST>
 __global__ void __launch_bounds__(kThreads) k_fock_rho_part(const __grid_constant__ FockParams p) {
+  if (p.active && !*p.active) return;
   using SC = cpx_t<ST>;
   __shared__ double2 red[kThreads];
   const int N = p.nk2, LS = p.LS;
@@ -241,6 +244,7 @@ __global__ void __launch_bounds__(kThreads) k_fock_rho_part(const __grid_constan
 
 template <typename ST, typename FT>
 __global__ void __launch_bounds__(kThreads) k_fock_col(const __grid_constant__ FockParams p) {
+  if (p.active && !*p.active) return;
   using SC = cpx_t<ST>;
   using FC = cpx_t<FT>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -289,6 +293,7 @@ __global__ void __launch_bounds__(kThreads) k_fock_col(const __grid_constant__ F
 // Reduces rho partials and forms the k-independent terms (fock.py:66-92).
 template <typename ST>
 __global__ void k_fock_consts(const __grid_constant__ FockParams p) {
+  if (p.active && !*p.active) return;
   using SC = cpx_t<ST>;
   __shared__ double2 rho[kMaxNb * kMaxNb];
   const int nb = p.nb, nb2 = p.nb2, LS = p.LS, ns = p.ngroups * LS;
@@ -353,6 +358,7 @@ __global__ void k_fock_consts(const __grid_constant__ FockParams p) {
 
 template <typename ST, typename FT>
 __global__ void __launch_bounds__(kThreads) k_fock_row_inv(const __grid_constant__ FockParams p) {
+  if (p.active && !*p.active) return;
   using SC = cpx_t<ST>;
   using FC = cpx_t<FT>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -491,11 +497,29 @@ extern "C" int hf_fock_workspace_size(int dtype, unsigned flags, int nk1, int nk
   return HF_OK;
 }
 
+namespace hf {
+int fock_build_internal(void* stream, int dtype, unsigned flags, int nk1, int nk2, int nb, const void* P,
+                        const void* h, const void* VR, const void* refP, const void* HH, const void* w2d,
+                        int n_contact, const void* contact_g, const void* contact_Oi, const void* contact_Oj,
+                        void* Sigma, void* H, void* F, void* workspace, size_t workspace_bytes,
+                        const int* active);
+}
+
 extern "C" int hf_fock_build(void* stream, int dtype, unsigned flags, int nk1, int nk2, int nb,
                              const void* P, const void* h, const void* VR, const void* refP,
                              const void* HH, const void* w2d, int n_contact, const void* contact_g,
                              const void* contact_Oi, const void* contact_Oj, void* Sigma, void* H,
                              void* F, void* workspace, size_t workspace_bytes) {
+  return hf::fock_build_internal(stream, dtype, flags, nk1, nk2, nb, P, h, VR, refP, HH, w2d, n_contact,
+                                 contact_g, contact_Oi, contact_Oj, Sigma, H, F, workspace, workspace_bytes,
+                                 nullptr);
+}
+
+int hf::fock_build_internal(void* stream, int dtype, unsigned flags, int nk1, int nk2, int nb, const void* P,
+                            const void* h, const void* VR, const void* refP, const void* HH, const void* w2d,
+                            int n_contact, const void* contact_g, const void* contact_Oi,
+                            const void* contact_Oj, void* Sigma, void* H, void* F, void* workspace,
+                            size_t workspace_bytes, const int* active) {
   int st = validate(dtype, flags, nk1, nk2, nb);
   if (st) return st;
   const bool exch = (flags & HF_FOCK_EXCHANGE) != 0;
@@ -525,6 +549,7 @@ extern "C" int hf_fock_build(void* stream, int dtype, unsigned flags, int nk1, i
   p.P = P; p.h = h; p.VR = VR; p.refP = refP; p.w2d = w2d; p.HH = HH;
   p.cg = contact_g; p.cOi = contact_Oi; p.cOj = contact_Oj;
   p.Sigma = Sigma; p.F = F; p.Hout = H;
+  p.active = active;
   char* ws = static_cast<char*>(workspace);
   p.scratch = ws + wl.scratch;
   const bool need_consts = (flags & HF_FOCK_HARTREE) || n_contact > 0;
@@ -536,7 +561,7 @@ extern "C" int hf_fock_build(void* stream, int dtype, unsigned flags, int nk1, i
   std::copy(sp.chan.begin(), sp.chan.end(), p.chan);
   std::copy(sp.partner.begin(), sp.partner.end(), p.partner);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (H && !need_consts) {
+  if (H && !need_consts && !active) {
     const size_t hb = (size_t)nb * nb * (dtype == HF_C128 ? sizeof(double2) : sizeof(float2));
     HF_CUDA(cudaMemsetAsync(H, 0, hb, s));
   }

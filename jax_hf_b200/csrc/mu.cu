@@ -33,6 +33,7 @@ struct MuArgs {
   double target, T;
   const double* mu0;
   double* out;
+  const int* active;  // optional device flag: return at once when *active == 0
 };
 
 template <typename RT>
@@ -100,6 +101,7 @@ __device__ __forceinline__ double expit(double x) { return 1.0 / (1.0 + exp(-x))
 
 template <typename RT>
 __global__ void __launch_bounds__(kMuThreads) k_find_mu(const MuArgs a) {
+  if (a.active && !*a.active) return;  // uniform across the cluster: no barrier is skipped by a subset
   cg::cluster_group cl = cg::this_cluster();
   __shared__ double slots[3][2];
   __shared__ double wsm[64];
@@ -190,9 +192,22 @@ __global__ void __launch_bounds__(kMuThreads) k_find_mu(const MuArgs a) {
 
 using namespace hf;
 
+namespace hf {
+int find_mu_internal(void* stream, int dtype, int method, int nk1, int nk2, int nb, const void* eps,
+                     const void* weights, double n_electrons, double T, int maxiter, const double* mu0,
+                     double* mu_out, const int* active);
+}
+
 extern "C" int hf_find_mu(void* stream, int dtype, int method, int nk1, int nk2, int nb,
                           const void* eps, const void* weights, double n_electrons, double T,
                           int maxiter, const double* mu0, double* mu_out) {
+  return hf::find_mu_internal(stream, dtype, method, nk1, nk2, nb, eps, weights, n_electrons, T, maxiter, mu0,
+                              mu_out, nullptr);
+}
+
+int hf::find_mu_internal(void* stream, int dtype, int method, int nk1, int nk2, int nb, const void* eps,
+                         const void* weights, double n_electrons, double T, int maxiter, const double* mu0,
+                         double* mu_out, const int* active) {
   if (dtype != HF_C128 && dtype != HF_C64) return fail(HF_ERR_INVALID, "bad dtype");
   if (method < 0 || method > 2) return fail(HF_ERR_INVALID, "method must be 0, 1 or 2");
   if (nk1 < 1 || nk2 < 1 || nb < 1) return fail(HF_ERR_INVALID, "bad shape");
@@ -206,7 +221,7 @@ extern "C" int hf_find_mu(void* stream, int dtype, int method, int nk1, int nk2,
   MuArgs a;
   a.eps = eps; a.w = weights;
   a.n = nk1 * nk2 * nb; a.nb = nb; a.method = method; a.maxiter = maxiter;
-  a.target = n_electrons; a.T = T; a.mu0 = mu0; a.out = mu_out;
+  a.target = n_electrons; a.T = T; a.mu0 = mu0; a.out = mu_out; a.active = active;
   int csize = (a.n + 4 * kMuThreads - 1) / (4 * kMuThreads);
   if (csize < 1) csize = 1;
   if (csize > kMuMaxCluster) csize = kMuMaxCluster;

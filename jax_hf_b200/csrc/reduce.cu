@@ -18,7 +18,8 @@ static int red_blocks(size_t n) {
 }
 
 __global__ void k_red_final(const double* __restrict__ part, int nparts, int mode, double T,
-                            const double* __restrict__ E, double* __restrict__ out) {
+                            const double* __restrict__ E, double* __restrict__ out, const int* active) {
+  if (active && !*active) return;
   __shared__ double sm[64];
   KSum acc;
   for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
@@ -38,7 +39,8 @@ template <typename RT>
 __global__ void __launch_bounds__(kRedThreads)
 k_energy_part(int nk, int nb, const cpx_t<RT>* __restrict__ P, const cpx_t<RT>* __restrict__ h,
               const cpx_t<RT>* __restrict__ S, const cpx_t<RT>* __restrict__ H, int H_mode,
-              const RT* __restrict__ w, double* __restrict__ part) {
+              const RT* __restrict__ w, double* __restrict__ part, const int* active) {
+  if (active && !*active) return;
   __shared__ double sm[64];
   const int nb2 = nb * nb;
   const size_t n = (size_t)nk * nb2;
@@ -95,9 +97,22 @@ extern "C" int hf_reduce_workspace_size(int nk1, int nk2, int nb, size_t* bytes)
   return HF_OK;
 }
 
+namespace hf {
+int energy_internal(void* stream, int dtype, int nk1, int nk2, int nb, const void* P, const void* h,
+                    const void* Sigma, const void* H, int H_mode, const void* w2d, double* E_out,
+                    void* workspace, size_t workspace_bytes, const int* active);
+}
+
 extern "C" int hf_energy(void* stream, int dtype, int nk1, int nk2, int nb, const void* P,
                          const void* h, const void* Sigma, const void* H, int H_mode,
                          const void* w2d, double* E_out, void* workspace, size_t workspace_bytes) {
+  return hf::energy_internal(stream, dtype, nk1, nk2, nb, P, h, Sigma, H, H_mode, w2d, E_out, workspace,
+                             workspace_bytes, nullptr);
+}
+
+int hf::energy_internal(void* stream, int dtype, int nk1, int nk2, int nb, const void* P, const void* h,
+                        const void* Sigma, const void* H, int H_mode, const void* w2d, double* E_out,
+                        void* workspace, size_t workspace_bytes, const int* active) {
   if (dtype != HF_C128 && dtype != HF_C64) return fail(HF_ERR_INVALID, "bad dtype");
   if (nk1 < 1 || nk2 < 1 || nb < 1) return fail(HF_ERR_INVALID, "bad shape");
   if (!P || !h || !Sigma || !w2d || !E_out) return fail(HF_ERR_INVALID, "NULL argument");
@@ -111,13 +126,13 @@ extern "C" int hf_energy(void* stream, int dtype, int nk1, int nk2, int nb, cons
   if (dtype == HF_C128)
     k_energy_part<double><<<nbk, kRedThreads, 0, s>>>(nk, nb, (const double2*)P, (const double2*)h,
                                                       (const double2*)Sigma, (const double2*)H, H_mode,
-                                                      (const double*)w2d, part);
+                                                      (const double*)w2d, part, active);
   else
     k_energy_part<float><<<nbk, kRedThreads, 0, s>>>(nk, nb, (const float2*)P, (const float2*)h,
                                                      (const float2*)Sigma, (const float2*)H, H_mode,
-                                                     (const float*)w2d, part);
+                                                     (const float*)w2d, part, active);
   HF_LAUNCH_CHECK("k_energy_part");
-  k_red_final<<<1, 256, 0, s>>>(part, nbk, 0, 0.0, nullptr, E_out);
+  k_red_final<<<1, 256, 0, s>>>(part, nbk, 0, 0.0, nullptr, E_out, active);
   HF_LAUNCH_CHECK("k_red_final");
   return HF_OK;
 }
@@ -139,7 +154,7 @@ static int entropy_common(void* stream, int dtype, int nk1, int nk2, int nb, con
   else
     k_entropy_part<float><<<nbk, kRedThreads, 0, s>>>(nk, nb, (const float*)p, (const float*)w_norm, part);
   HF_LAUNCH_CHECK("k_entropy_part");
-  k_red_final<<<1, 256, 0, s>>>(part, nbk, mode, T, E, out);
+  k_red_final<<<1, 256, 0, s>>>(part, nbk, mode, T, E, out, nullptr);
   HF_LAUNCH_CHECK("k_red_final");
   return HF_OK;
 }

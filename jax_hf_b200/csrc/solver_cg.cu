@@ -1,0 +1,767 @@
+// Direct-minimisation solver on the device: preconditioned Riemannian CG on
+// Stiefel x capped simplex with the spectral Cayley line search
+// (solver.py:307-660).  All state and every scalar of the loop (mu, energy,
+// gradient norm, PR beta, step, line-search decision, history, stopping rule)
+// live in device memory; the host only enqueues kernels and reads one flag per
+// chunk of iterations.
+//
+// One iteration = density -> Fock build (3 FFT passes) -> energy -> grad1 ->
+// grad2 -> direction (+ Jacobi eigh of i d_Q) -> first trial -> remaining
+// trials -> retraction -> mu -> step end.  Per-k kernels run one warp per
+// k-point; each reduction is finalised by the last CTA to finish (atomic
+// ticket), which also performs the scalar update of the reference loop body.
+// Every kernel of an iteration returns at once when the device flag `active`
+// is clear, so whole chunks can be queued without host round trips.
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+#include "perk.cuh"
+#include "solver_common.cuh"
+
+namespace hf {
+
+int fock_build_internal(void* stream, int dtype, unsigned flags, int nk1, int nk2, int nb, const void* P,
+                        const void* h, const void* VR, const void* refP, const void* HH, const void* w2d,
+                        int n_contact, const void* contact_g, const void* contact_Oi, const void* contact_Oj,
+                        void* Sigma, void* H, void* F, void* workspace, size_t workspace_bytes,
+                        const int* active);
+int energy_internal(void* stream, int dtype, int nk1, int nk2, int nb, const void* P, const void* h,
+                    const void* Sigma, const void* H, int H_mode, const void* w2d, double* E_out,
+                    void* workspace, size_t workspace_bytes, const int* active);
+int find_mu_internal(void* stream, int dtype, int method, int nk1, int nk2, int nb, const void* eps,
+                     const void* weights, double n_electrons, double T, int maxiter, const double* mu0,
+                     double* mu_out, const int* active);
+
+struct CgScalars {
+  int k, active, accepted, converged, k_base, pad_;
+  double mu, E, E_prev, dE, grad_norm;
+  double lam, pr_den, beta, tau0, tau_final, Omega0, E_fin;
+};
+
+struct CgArgs {
+  int nk, nb, max_iter, cg_restart, bt_max, plateau_window;
+  double T_r, tol_E, tol_grad, denom_scale, max_step, bt_shrink, n_target_norm;
+  double2 *Q, *P, *F, *Ft, *G0, *G1, *dQ, *Vd, *Fe;
+  double *p, *eps, *epsF, *gp0, *gp1, *dp, *lamd, *w_norm;
+  double* hist_E;
+  double* hist_G;
+  CgScalars* sc;
+  double* part;
+  unsigned* counter;
+};
+
+__device__ __forceinline__ bool cg_active(const CgArgs& a) { return a.sc->active != 0; }
+
+// ------------------------------------------------------------------ init ---
+__global__ void k_cg_init(CgArgs a, const double2* __restrict__ P0, const double* __restrict__ w2d,
+                          double weight_sum) {
+  const size_t nb2 = (size_t)a.nb * a.nb;
+  const size_t nq = (size_t)a.nk * nb2, nv = (size_t)a.nk * a.nb;
+  const double ws = fmax(weight_sum, 1e-30);
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < nq; e += (size_t)gridDim.x * blockDim.x) {
+    const size_t k = e / nb2;
+    const int r = (int)(e - k * nb2), i = r / a.nb, j = r - (r / a.nb) * a.nb;
+    const double2 x = P0[e], y = P0[k * nb2 + (size_t)j * a.nb + i];
+    a.P[e] = make_double2(0.5 * (x.x + y.x), 0.5 * (x.y - y.y));
+    a.G0[e] = a.G1[e] = a.dQ[e] = make_double2(0.0, 0.0);
+  }
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < nv; e += (size_t)gridDim.x * blockDim.x)
+    a.gp0[e] = a.gp1[e] = a.dp[e] = 0.0;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < (size_t)a.nk; k += (size_t)gridDim.x * blockDim.x)
+    a.w_norm[k] = w2d[k] / ws;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    CgScalars* s = a.sc;
+    s->k = 0;
+    s->k_base = 0;
+    s->active = a.max_iter > 0 ? 1 : 0;
+    s->accepted = 0;
+    s->converged = 0;
+    s->mu = 0.0;
+    s->E = 0.0;
+    s->E_prev = INFINITY;
+    s->dE = INFINITY;
+    s->grad_norm = INFINITY;
+    s->lam = s->pr_den = s->beta = s->tau0 = s->tau_final = s->Omega0 = s->E_fin = 0.0;
+    *a.counter = 0u;
+  }
+}
+
+// eps, Q <- eigh(A) per k (A = F0 at init, or Ft = Q^H F Q at finalize with Q <- Q V)
+__global__ void k_cg_eig(CgArgs a, const double2* __restrict__ A, int rotate) {
+  extern __shared__ double2 sm[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  const int nb = a.nb, nb2 = nb * nb;
+  double2* m = sm + (size_t)w * (jacobi_smem_elems(nb) + 2 * nb2);
+  double2* v = m + nb2;
+  double2* scr = v + nb2;
+  double2* q = scr + nb + 40;
+  double2* t = q + nb2;
+  double* wv = reinterpret_cast<double*>(scr);
+  for (int k = blockIdx.x * wpb + w; k < a.nk; k += gridDim.x * wpb) {
+    const size_t base = (size_t)k * nb2;
+    if (rotate) {
+      for (int e = lane; e < nb2; e += 32) { q[e] = a.Q[base + e]; m[e] = A[base + e]; }
+      __syncwarp();
+      warp_qhaq(q, m, t, nb, lane);  // m <- Q^H F Q
+      __syncwarp();
+    } else {
+      for (int e = lane; e < nb2; e += 32) m[e] = A[base + e];
+      __syncwarp();
+    }
+    // hermitise (jnp.linalg.eigh symmetrises its input)
+    for (int e = lane; e < nb2; e += 32) {
+      const int i = e / nb, j = e - i * nb;
+      if (i < j) {
+        const double2 x = m[e], y = m[j * nb + i];
+        const double2 hxy = make_double2(0.5 * (x.x + y.x), 0.5 * (x.y - y.y));
+        m[e] = hxy;
+        m[j * nb + i] = conj(hxy);
+      } else if (i == j) {
+        m[e].y = 0.0;
+      }
+    }
+    __syncwarp();
+    warp_jacobi_eigh(m, v, scr + nb, nb, lane, 1e-17);
+    for (int e = lane; e < nb; e += 32) wv[e] = m[e * nb + e].x;
+    __syncwarp();
+    for (int i = lane; i < nb; i += 32) {
+      const double wi = wv[i];
+      int r = 0;
+      for (int j = 0; j < nb; ++j) r += (wv[j] < wi) || (wv[j] == wi && j < i);
+      a.eps[(size_t)k * nb + r] = wi;
+      for (int row = 0; row < nb; ++row) t[row * nb + r] = v[row * nb + i];
+    }
+    __syncwarp();
+    if (rotate) {  // Q <- Q V
+      for (int e = lane; e < nb2; e += 32) {
+        const int i = e / nb, j = e - i * nb;
+        double2 acc = make_double2(0.0, 0.0);
+        for (int n = 0; n < nb; ++n) acc = cadd(acc, cmul(q[i * nb + n], t[n * nb + j]));
+        a.Q[base + e] = acc;
+      }
+    } else {
+      for (int e = lane; e < nb2; e += 32) a.Q[base + e] = t[e];
+    }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------- density: p and P = herm(Q p Q^H)
+__global__ void k_cg_density(CgArgs a, int force) {
+  if (!force && !cg_active(a)) return;
+  extern __shared__ double2 sm[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  const int nb = a.nb, nb2 = nb * nb;
+  double2* q = sm + (size_t)w * (2 * nb2 + nb);
+  double2* t = q + nb2;
+  double* pp = reinterpret_cast<double*>(t + nb2);
+  const double mu = a.sc->mu;
+  for (int k = blockIdx.x * wpb + w; k < a.nk; k += gridDim.x * wpb) {
+    const size_t base = (size_t)k * nb2;
+    for (int e = lane; e < nb2; e += 32) q[e] = a.Q[base + e];
+    for (int i = lane; i < nb; i += 32) {
+      const double pv = sigmoid((mu - a.eps[(size_t)k * nb + i]) / a.T_r);
+      pp[i] = pv;
+      a.p[(size_t)k * nb + i] = pv;
+    }
+    __syncwarp();
+    warp_density(q, pp, t, nb, lane);
+    __syncwarp();
+    for (int e = lane; e < nb2; e += 32) {
+      const int i = e / nb, j = e - i * nb;
+      const double2 x = t[e], y = t[j * nb + i];
+      a.P[base + e] = make_double2(0.5 * (x.x + y.x), 0.5 * (x.y - y.y));
+    }
+    __syncwarp();
+  }
+}
+
+// ----------------------------------- grad1: Ft, eps, G, g_p and four norms ---
+__global__ void k_cg_grad1(CgArgs a) {
+  if (!cg_active(a)) return;
+  extern __shared__ double2 sm[];
+  __shared__ double red[64];
+  __shared__ double tot[kMaxSums];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  const int nb = a.nb, nb2 = nb * nb;
+  double2* q = sm + (size_t)w * 3 * nb2;
+  double2* f = q + nb2;
+  double2* t = f + nb2;
+  const int par = a.sc->k & 1;
+  double2* G = par ? a.G1 : a.G0;
+  const double2* Gp = par ? a.G0 : a.G1;
+  double* gp = par ? a.gp1 : a.gp0;
+  const double* gpp = par ? a.gp0 : a.gp1;
+  const double mu = a.sc->mu;
+  KSum acc[4];
+  for (int k = blockIdx.x * wpb + w; k < a.nk; k += gridDim.x * wpb) {
+    const size_t base = (size_t)k * nb2, vb = (size_t)k * nb;
+    const double wk = a.w_norm[k];
+    for (int e = lane; e < nb2; e += 32) { q[e] = a.Q[base + e]; f[e] = a.F[base + e]; }
+    __syncwarp();
+    warp_qhaq(q, f, t, nb, lane);
+    __syncwarp();
+    for (int e = lane; e < nb2; e += 32) {
+      const int i = e / nb, j = e - i * nb;
+      const double2 ft = f[e];
+      a.Ft[base + e] = ft;
+      double2 g = make_double2(0.0, 0.0);
+      if (i != j) {
+        const double2 fji = f[j * nb + i];
+        const double dpij = a.p[vb + j] - a.p[vb + i];
+        g = make_double2(0.5 * dpij * (ft.x + fji.x), 0.5 * dpij * (ft.y - fji.y));
+      }
+      G[base + e] = g;
+      acc[0].add(wk * (g.x * g.x + g.y * g.y));
+      const double2 o = Gp[base + e];
+      acc[2].add(wk * (o.x * o.x + o.y * o.y));
+    }
+    for (int i = lane; i < nb; i += 32) {
+      const double ei = f[i * nb + i].x;
+      a.epsF[vb + i] = ei;
+      const double ps = clip(a.p[vb + i], 1e-6, 1.0 - 1e-6);
+      const double g = ei + a.T_r * (log(ps) - log1p(-ps)) - mu;
+      gp[vb + i] = g;
+      acc[1].add(ei * ei);
+      acc[3].add(wk * gpp[vb + i] * gpp[vb + i]);
+    }
+    __syncwarp();
+  }
+  if (publish_partials<4>(acc, a.part, a.counter, red)) {
+    gather_partials<4>(a.part, a.counter, tot);
+    if (threadIdx.x == 0) {
+      CgScalars* s = a.sc;
+      s->grad_norm = sqrt(fmax(0.0, tot[0]));
+      const double eps_scale = sqrt(tot[1] / ((double)a.nk * a.nb) + 1e-30);
+      s->lam = fmax(a.T_r, a.denom_scale * eps_scale);
+      s->pr_den = tot[2] + tot[3];
+    }
+  }
+}
+
+__device__ __forceinline__ double2 precond(double2 g, double ei, double ej, double lam) {
+  const double gap = ei - ej;
+  const double d = sqrt(gap * gap + lam * lam);
+  return make_double2(g.x / d, g.y / d);
+}
+
+// --------------------------------------------- grad2: PR+ inner products ---
+__global__ void k_cg_grad2(CgArgs a) {
+  if (!cg_active(a)) return;
+  __shared__ double red[64];
+  __shared__ double tot[kMaxSums];
+  const int par = a.sc->k & 1;
+  const double2* G = par ? a.G1 : a.G0;
+  const double2* Gp = par ? a.G0 : a.G1;
+  const double* gp = par ? a.gp1 : a.gp0;
+  const double* gpp = par ? a.gp0 : a.gp1;
+  const double lam = a.sc->lam;
+  const int nb = a.nb, nb2 = nb * nb;
+  const size_t nq = (size_t)a.nk * nb2;
+  KSum acc[4];
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < nq; e += (size_t)gridDim.x * blockDim.x) {
+    const size_t k = e / nb2;
+    const int r = (int)(e - k * nb2), i = r / nb, j = r - (r / nb) * nb;
+    const double wk = a.w_norm[k];
+    const double2 g = G[e];
+    const double2 hq = precond(g, a.epsF[k * nb + i], a.epsF[k * nb + j], lam);
+    const double2 o = Gp[e];
+    acc[0].add(wk * (g.x * hq.x + g.y * hq.y));
+    acc[1].add(wk * (o.x * hq.x + o.y * hq.y));
+    if (j == 0) {
+      const size_t vi = k * nb + i;
+      const double ps = clip(a.p[vi], 1e-8, 1.0 - 1e-8);
+      const double hp = gp[vi] * (ps * (1.0 - ps) / a.T_r);
+      acc[2].add(wk * gp[vi] * hp);
+      acc[3].add(wk * gpp[vi] * hp);
+    }
+  }
+  if (publish_partials<4>(acc, a.part, a.counter, red)) {
+    gather_partials<4>(a.part, a.counter, tot);
+    if (threadIdx.x == 0) {
+      CgScalars* s = a.sc;
+      const double num = tot[0] - tot[1] + tot[2] - tot[3];
+      double beta = s->pr_den > 1e-30 ? fmax(0.0, num / s->pr_den) : 0.0;
+      beta = fmin(beta, 5.0);
+      if (s->k == 0 || s->k % a.cg_restart == 0) beta = 0.0;
+      s->beta = beta;
+    }
+  }
+}
+
+// ---- direction d = H + beta d_prev, eigh(i d) -> (V, lam), Fe = V^H Ft V, tau0, Omega0
+__global__ void k_cg_dir(CgArgs a) {
+  if (!cg_active(a)) return;
+  extern __shared__ double2 sm[];
+  __shared__ double red[64];
+  __shared__ double tot[kMaxSums];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  const int nb = a.nb, nb2 = nb * nb;
+  double2* m = sm + (size_t)w * (jacobi_smem_elems(nb) + 2 * nb2);
+  double2* v = m + nb2;
+  double2* scr = v + nb2;
+  double2* ft = scr + nb + 40;
+  double2* t = ft + nb2;
+  double* wv = reinterpret_cast<double*>(scr);
+  const int par = a.sc->k & 1;
+  const double2* G = par ? a.G1 : a.G0;
+  const double* gp = par ? a.gp1 : a.gp0;
+  const double lam = a.sc->lam, beta = a.sc->beta;
+  const double Tm = fmax(a.T_r, 1e-14);
+  (void)Tm;
+  KSum acc[3];
+  for (int k = blockIdx.x * wpb + w; k < a.nk; k += gridDim.x * wpb) {
+    const size_t base = (size_t)k * nb2, vb = (size_t)k * nb;
+    const double wk = a.w_norm[k];
+    for (int e = lane; e < nb2; e += 32) {
+      const int i = e / nb, j = e - i * nb;
+      const double2 hq = precond(G[base + e], a.epsF[vb + i], a.epsF[vb + j], lam);
+      const double2 dprev = a.dQ[base + e];
+      const double2 d = make_double2(hq.x + beta * dprev.x, hq.y + beta * dprev.y);
+      a.dQ[base + e] = d;
+      t[e] = d;
+      acc[0].add(wk * (d.x * d.x + d.y * d.y));
+      ft[e] = a.Ft[base + e];
+    }
+    for (int i = lane; i < nb; i += 32) {
+      const double pv = a.p[vb + i];
+      const double ps = clip(pv, 1e-8, 1.0 - 1e-8);
+      const double hp = gp[vb + i] * (ps * (1.0 - ps) / a.T_r);
+      a.dp[vb + i] = hp + beta * a.dp[vb + i];
+      acc[1].add(wk * ps * a.epsF[vb + i]);
+      acc[2].add(wk * ent_term(ps));
+    }
+    __syncwarp();
+    // m = herm(i d)
+    for (int e = lane; e < nb2; e += 32) {
+      const int i = e / nb, j = e - i * nb;
+      const double2 x = mul_pi(t[e]), y = mul_pi(t[j * nb + i]);
+      m[e] = make_double2(0.5 * (x.x + y.x), 0.5 * (x.y - y.y));
+    }
+    __syncwarp();
+    warp_jacobi_eigh(m, v, scr + nb, nb, lane, 1e-17);
+    for (int e = lane; e < nb; e += 32) wv[e] = m[e * nb + e].x;
+    __syncwarp();
+    for (int i = lane; i < nb; i += 32) {  // ascending order, V columns
+      const double wi = wv[i];
+      int r = 0;
+      for (int j = 0; j < nb; ++j) r += (wv[j] < wi) || (wv[j] == wi && j < i);
+      a.lamd[vb + r] = wi;
+      for (int row = 0; row < nb; ++row) t[row * nb + r] = v[row * nb + i];
+    }
+    __syncwarp();
+    for (int e = lane; e < nb2; e += 32) a.Vd[base + e] = t[e];
+    warp_qhaq(t, ft, m, nb, lane);  // ft <- V^H Ft V
+    __syncwarp();
+    for (int e = lane; e < nb2; e += 32) a.Fe[base + e] = ft[e];
+    __syncwarp();
+  }
+  if (publish_partials<3>(acc, a.part, a.counter, red)) {
+    gather_partials<3>(a.part, a.counter, tot);
+    if (threadIdx.x == 0) {
+      CgScalars* s = a.sc;
+      const double dn = sqrt(fmax(0.0, tot[0]));
+      s->tau0 = fmin(1.0, a.max_step / fmax(dn, 1e-30));
+      s->Omega0 = tot[1] + fmax(a.T_r, 1e-14) * tot[2];
+      s->accepted = 0;
+      s->tau_final = s->tau0;
+    }
+  }
+}
+
+// -------------------- line-search trials i0 <= i < i1 on the frozen-F free energy
+template <int NT>
+__global__ void k_cg_trials(CgArgs a, int i0, int i1, int last_chunk) {
+  if (!cg_active(a)) return;
+  if (a.sc->accepted) return;
+  extern __shared__ double2 sm[];
+  __shared__ double red[64];
+  __shared__ double tot[kMaxSums];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  const int nb = a.nb, nb2 = nb * nb;
+  double2* v = sm + (size_t)w * (2 * nb2 + nb);
+  double2* f = v + nb2;
+  double2* c = f + nb2;
+  const int nt = i1 - i0;
+  double taus[NT];
+  {
+    double tau = a.sc->tau0;
+    for (int i = 0; i < i0; ++i) tau = tau * a.bt_shrink;
+    for (int i = 0; i < NT; ++i) { taus[i] = tau; tau = tau * a.bt_shrink; }
+  }
+  KSum acc[2 * NT];
+  for (int k = blockIdx.x * wpb + w; k < a.nk; k += gridDim.x * wpb) {
+    const size_t base = (size_t)k * nb2, vb = (size_t)k * nb;
+    const double wk = a.w_norm[k];
+    for (int e = lane; e < nb2; e += 32) { v[e] = a.Vd[base + e]; f[e] = a.Fe[base + e]; }
+    for (int it = 0; it < nt; ++it) {
+      __syncwarp();
+      for (int i = lane; i < nb; i += 32) c[i] = cayley_factor(taus[it], a.lamd[vb + i]);
+      __syncwarp();
+      for (int i = lane; i < nb; i += 32) {
+        const double et = diag_ufu_row(v, f, c, nb, i);
+        const double pt = clip(a.p[vb + i] - taus[it] * a.dp[vb + i], 1e-8, 1.0 - 1e-8);
+        acc[2 * it].add(wk * pt * et);
+        acc[2 * it + 1].add(wk * ent_term(pt));
+      }
+    }
+    __syncwarp();
+  }
+  if (publish_partials<2 * NT>(acc, a.part, a.counter, red)) {
+    gather_partials<2 * NT>(a.part, a.counter, tot);
+    if (threadIdx.x == 0) {
+      CgScalars* s = a.sc;
+      const double Tm = fmax(a.T_r, 1e-14);
+      for (int it = 0; it < nt; ++it) {
+        const double om = tot[2 * it] + Tm * tot[2 * it + 1];
+        if (om < s->Omega0) { s->accepted = 1; s->tau_final = taus[it]; break; }
+      }
+      if (!s->accepted && last_chunk) s->tau_final = s->tau0 * pow(a.bt_shrink, (double)a.bt_max);
+    }
+  }
+}
+
+// ----------------- retraction: U(tau), Q <- Q U, eps_new = diag(U^H Ft U)
+__global__ void k_cg_update(CgArgs a) {
+  if (!cg_active(a)) return;
+  extern __shared__ double2 sm[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  const int nb = a.nb, nb2 = nb * nb;
+  double2* v = sm + (size_t)w * (4 * nb2 + nb);
+  double2* f = v + nb2;
+  double2* u = f + nb2;
+  double2* q = u + nb2;
+  double2* c = q + nb2;
+  const double tau = a.sc->tau_final;
+  for (int k = blockIdx.x * wpb + w; k < a.nk; k += gridDim.x * wpb) {
+    const size_t base = (size_t)k * nb2, vb = (size_t)k * nb;
+    for (int e = lane; e < nb2; e += 32) { v[e] = a.Vd[base + e]; f[e] = a.Fe[base + e]; q[e] = a.Q[base + e]; }
+    for (int i = lane; i < nb; i += 32) c[i] = cayley_factor(tau, a.lamd[vb + i]);
+    __syncwarp();
+    for (int e = lane; e < nb2; e += 32) {
+      const int i = e / nb, j = e - i * nb;
+      double2 acc = make_double2(0.0, 0.0);
+      for (int n = 0; n < nb; ++n) acc = cadd(acc, cmulc(cmul(v[i * nb + n], c[n]), v[j * nb + n]));
+      u[e] = acc;
+    }
+    for (int i = lane; i < nb; i += 32) a.eps[vb + i] = diag_ufu_row(v, f, c, nb, i);
+    __syncwarp();
+    for (int e = lane; e < nb2; e += 32) {
+      const int i = e / nb, j = e - i * nb;
+      double2 acc = make_double2(0.0, 0.0);
+      for (int n = 0; n < nb; ++n) acc = cadd(acc, cmul(q[i * nb + n], u[n * nb + j]));
+      a.Q[base + e] = acc;
+    }
+    __syncwarp();
+  }
+}
+
+// ------------------------------- history, |dE| and the stopping rule ---
+// solver.py:422-449 and 595-597.  `phase_rel` > 0 only in the FP32-exchange
+// phase of the mixed solve: the energy tolerance is raised to the FP32 noise
+// floor phase_rel |E|; k_base restarts the plateau window at the FP64 switch
+// (k_base = 0 reproduces the reference rule exactly).
+__global__ void k_cg_step_end(CgArgs a, double phase_rel) {
+  if (!cg_active(a)) return;
+  CgScalars* s = a.sc;
+  const int k = s->k;
+  a.hist_E[k] = s->E;
+  a.hist_G[k] = s->grad_norm;
+  s->dE = fabs(s->E - s->E_prev);
+  s->E_prev = s->E;
+  const int kn = k + 1;
+  s->k = kn;
+  const double tol = phase_rel > 0.0 ? fmax(a.tol_E, phase_rel * fabs(s->E)) : a.tol_E;
+  const int kk = kn - s->k_base;
+  bool enc;
+  if (a.plateau_window > 0) {
+    const double e_now = a.hist_E[max(kn - 1, 0)];
+    const double e_past = a.hist_E[max(kn - 1 - a.plateau_window, s->k_base)];
+    enc = (kk > a.plateau_window) ? (e_past - e_now) > tol : s->dE > tol;
+  } else {
+    enc = s->dE > tol;
+  }
+  const bool nc = a.tol_grad > 0.0 ? s->grad_norm > a.tol_grad : enc;
+  s->active = (kn < a.max_iter && nc) ? 1 : 0;
+}
+
+// FP32 -> FP64 switch of the mixed solve: continue from the current state.
+__global__ void k_cg_rearm(CgArgs a) {
+  CgScalars* s = a.sc;
+  s->k_base = s->k;
+  s->active = s->k < a.max_iter ? 1 : 0;
+}
+
+__global__ void k_cg_converged(CgArgs a) {
+  CgScalars* s = a.sc;
+  s->converged = a.tol_grad > 0.0 ? (s->grad_norm <= a.tol_grad) : (s->k < a.max_iter);
+}
+
+// ============================================================ host driver ===
+struct CgLayout {
+  size_t off[24];
+  size_t total;
+};
+
+static size_t cg_layout(const hf_cg_problem& pb, size_t fock_ws, size_t red_ws, CgLayout& L) {
+  const size_t nk = (size_t)pb.nk1 * pb.nk2, nb = pb.nb, nq = nk * nb * nb, nv = nk * nb;
+  const size_t sizes[] = {
+      nq * 16, nq * 16, nq * 16, nq * 16, nq * 16, nq * 16, nq * 16,  // Ft G0 G1 dQ Vd Fe Sigma
+      nv * 8, nv * 8, nv * 8, nv * 8, nv * 8, nv * 8,                  // eps epsF gp0 gp1 dp lamd
+      nk * 8,                                                          // w_norm
+      nb * nb * 16,                                                    // H
+      sizeof(CgScalars), 64,                                           // scalars, counter
+      (size_t)148 * 16 * kMaxSums * 2 * 8,                             // partials
+      fock_ws, red_ws};
+  size_t o = 0;
+  const int n = sizeof(sizes) / sizeof(sizes[0]);
+  for (int i = 0; i < n; ++i) { L.off[i] = o; o += align_up(sizes[i], 256); }
+  L.total = o;
+  return o;
+}
+
+static int fock_ws_size(const hf_cg_problem& pb, unsigned fflags, size_t* out) {
+  return hf_fock_workspace_size(HF_C128, fflags, pb.nk1, pb.nk2, pb.nb, out);
+}
+
+static unsigned fock_flags(const hf_cg_problem& pb, bool fp32) {
+  unsigned f = pb.fock_flags & ~(unsigned)HF_FOCK_FFT_FP32;
+  if (fp32) f |= HF_FOCK_FFT_FP32;
+  return f;
+}
+
+struct CgRun {
+  const hf_cg_problem* pb;
+  CgArgs a;
+  void* fock_ws;
+  size_t fock_ws_bytes;
+  void* red_ws;
+  size_t red_ws_bytes;
+  double2* Sigma;
+  double2* H;
+  int nblk;
+};
+
+static size_t smem_eig(int nb) { return (jacobi_smem_elems(nb) + 2 * (size_t)nb * nb) * sizeof(double2) * kSolverWarps; }
+
+static int set_smem(const void* fn, size_t bytes) {
+  HF_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  return HF_OK;
+}
+
+static int cg_fock(CgRun& r, cudaStream_t s, bool fp32, const int* active) {
+  const hf_cg_problem& pb = *r.pb;
+  return fock_build_internal(s, HF_C128, fock_flags(pb, fp32), pb.nk1, pb.nk2, pb.nb, r.a.P, pb.h, pb.VR,
+                             pb.refP, pb.HH, pb.w2d, pb.n_contact, pb.contact_g, pb.contact_Oi, pb.contact_Oj,
+                             r.Sigma, r.H, r.a.F, r.fock_ws, r.fock_ws_bytes, active);
+}
+
+static int cg_energy(CgRun& r, cudaStream_t s, double* out, const int* active) {
+  const hf_cg_problem& pb = *r.pb;
+  return energy_internal(s, HF_C128, pb.nk1, pb.nk2, pb.nb, r.a.P, pb.h, r.Sigma, r.H, 1, pb.w2d, out, r.red_ws,
+                         r.red_ws_bytes, active);
+}
+
+static int cg_mu(CgRun& r, cudaStream_t s, int maxiter, const int* active) {
+  const hf_cg_problem& pb = *r.pb;
+  return find_mu_internal(s, HF_C128, 2, pb.nk1, pb.nk2, pb.nb, r.a.eps, r.a.w_norm, r.a.n_target_norm, r.a.T_r,
+                          maxiter, &r.a.sc->mu, &r.a.sc->mu, active);
+}
+
+static int cg_iteration(CgRun& r, cudaStream_t s, const hf_cg_config& cf, bool fp32) {
+  const double phase_rel = fp32 ? cf.fp32_switch_rel : 0.0;
+  const int nb = r.pb->nb, nb2 = nb * nb;
+  const int* act = &r.a.sc->active;
+  const dim3 blk(32 * kSolverWarps);
+  const size_t sm_den = (2 * (size_t)nb2 + nb) * 16 * kSolverWarps;
+  k_cg_density<<<r.nblk, blk, sm_den, s>>>(r.a, 0);
+  HF_LAUNCH_CHECK("k_cg_density");
+  int st = cg_fock(r, s, fp32, act);
+  if (st) return st;
+  st = cg_energy(r, s, &r.a.sc->E, act);
+  if (st) return st;
+  const size_t sm_g1 = 3 * (size_t)nb2 * 16 * kSolverWarps;
+  k_cg_grad1<<<r.nblk, blk, sm_g1, s>>>(r.a);
+  HF_LAUNCH_CHECK("k_cg_grad1");
+  k_cg_grad2<<<r.nblk, 256, 0, s>>>(r.a);
+  HF_LAUNCH_CHECK("k_cg_grad2");
+  k_cg_dir<<<r.nblk, blk, smem_eig(nb), s>>>(r.a);
+  HF_LAUNCH_CHECK("k_cg_dir");
+  const size_t sm_tr = (2 * (size_t)nb2 + nb) * 16 * kSolverWarps;
+  const int bt = cf.bt_max;
+  if (bt >= 1) {
+    k_cg_trials<1><<<r.nblk, blk, sm_tr, s>>>(r.a, 0, 1, bt == 1);
+    HF_LAUNCH_CHECK("k_cg_trials");
+    for (int i0 = 1; i0 < bt; i0 += 8) {
+      const int i1 = i0 + 8 < bt ? i0 + 8 : bt;
+      k_cg_trials<8><<<r.nblk, blk, sm_tr, s>>>(r.a, i0, i1, i1 == bt);
+      HF_LAUNCH_CHECK("k_cg_trials");
+    }
+  }
+  const size_t sm_up = (4 * (size_t)nb2 + nb) * 16 * kSolverWarps;
+  k_cg_update<<<r.nblk, blk, sm_up, s>>>(r.a);
+  HF_LAUNCH_CHECK("k_cg_update");
+  st = cg_mu(r, s, cf.mu_maxiter, act);
+  if (st) return st;
+  k_cg_step_end<<<1, 1, 0, s>>>(r.a, phase_rel);
+  HF_LAUNCH_CHECK("k_cg_step_end");
+  return HF_OK;
+}
+
+static int cg_check(const hf_cg_problem* pb, const hf_cg_config* cf) {
+  if (!pb || !cf) return fail(HF_ERR_INVALID, "NULL problem/config");
+  if (pb->nk1 < 1 || pb->nk2 < 1 || pb->nb < 1) return fail(HF_ERR_INVALID, "bad shape");
+  if (pb->nb > 16) return fail(HF_ERR_UNSUPPORTED, "the device CG solver supports nb <= 16");
+  if (cf->max_iter < 0 || cf->bt_max < 0 || cf->cg_restart < 1)
+    return fail(HF_ERR_INVALID, "bad solver configuration");
+  return HF_OK;
+}
+
+}  // namespace hf
+
+using namespace hf;
+
+extern "C" int hf_cg_workspace_size(const hf_cg_problem* pb, const hf_cg_config* cf, size_t* bytes) {
+  int st = cg_check(pb, cf);
+  if (st) return st;
+  size_t fws = 0, f2 = 0, rws = 0;
+  if ((st = fock_ws_size(*pb, fock_flags(*pb, false), &fws))) return st;
+  if ((st = fock_ws_size(*pb, fock_flags(*pb, true), &f2))) return st;
+  if ((st = hf_reduce_workspace_size(pb->nk1, pb->nk2, pb->nb, &rws))) return st;
+  CgLayout L;
+  *bytes = cg_layout(*pb, fws > f2 ? fws : f2, rws, L) + (size_t)cf->max_iter * 16 + 256;
+  return HF_OK;
+}
+
+extern "C" int hf_cg_solve(void* stream, const hf_cg_problem* pb, const hf_cg_config* cf, const void* P0,
+                           void* Q, void* p, void* density, void* fock, double* hist_E, double* hist_grad,
+                           double* scalars_out, void* workspace, size_t workspace_bytes) {
+  int st = cg_check(pb, cf);
+  if (st) return st;
+  if (!P0 || !Q || !p || !density || !fock || !scalars_out || !workspace)
+    return fail(HF_ERR_INVALID, "NULL argument");
+  size_t need = 0;
+  if ((st = hf_cg_workspace_size(pb, cf, &need))) return st;
+  if (workspace_bytes < need) return fail(HF_ERR_WORKSPACE, "CG workspace too small: need " + std::to_string(need));
+  size_t fws = 0, f2 = 0, rws = 0;
+  fock_ws_size(*pb, fock_flags(*pb, false), &fws);
+  fock_ws_size(*pb, fock_flags(*pb, true), &f2);
+  hf_reduce_workspace_size(pb->nk1, pb->nk2, pb->nb, &rws);
+  CgLayout L;
+  cg_layout(*pb, fws > f2 ? fws : f2, rws, L);
+  char* ws = static_cast<char*>(workspace);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+
+  CgRun r;
+  r.pb = pb;
+  CgArgs& a = r.a;
+  a.nk = pb->nk1 * pb->nk2;
+  a.nb = pb->nb;
+  a.max_iter = cf->max_iter;
+  a.cg_restart = cf->cg_restart;
+  a.bt_max = cf->bt_max;
+  a.plateau_window = cf->plateau_window;
+  a.T_r = fmax(pb->T, 1e-12);
+  a.tol_E = cf->tol_E;
+  a.tol_grad = cf->tol_grad;
+  a.denom_scale = cf->denom_scale;
+  a.max_step = cf->max_step;
+  a.bt_shrink = cf->bt_shrink;
+  a.n_target_norm = pb->n_electrons / fmax(pb->weight_sum, 1e-30);
+  a.Q = static_cast<double2*>(Q);
+  a.P = static_cast<double2*>(density);
+  a.F = static_cast<double2*>(fock);
+  a.p = static_cast<double*>(p);
+  a.Ft = reinterpret_cast<double2*>(ws + L.off[0]);
+  a.G0 = reinterpret_cast<double2*>(ws + L.off[1]);
+  a.G1 = reinterpret_cast<double2*>(ws + L.off[2]);
+  a.dQ = reinterpret_cast<double2*>(ws + L.off[3]);
+  a.Vd = reinterpret_cast<double2*>(ws + L.off[4]);
+  a.Fe = reinterpret_cast<double2*>(ws + L.off[5]);
+  r.Sigma = reinterpret_cast<double2*>(ws + L.off[6]);
+  a.eps = reinterpret_cast<double*>(ws + L.off[7]);
+  a.epsF = reinterpret_cast<double*>(ws + L.off[8]);
+  a.gp0 = reinterpret_cast<double*>(ws + L.off[9]);
+  a.gp1 = reinterpret_cast<double*>(ws + L.off[10]);
+  a.dp = reinterpret_cast<double*>(ws + L.off[11]);
+  a.lamd = reinterpret_cast<double*>(ws + L.off[12]);
+  a.w_norm = reinterpret_cast<double*>(ws + L.off[13]);
+  r.H = reinterpret_cast<double2*>(ws + L.off[14]);
+  a.sc = reinterpret_cast<CgScalars*>(ws + L.off[15]);
+  a.counter = reinterpret_cast<unsigned*>(ws + L.off[16]);
+  a.part = reinterpret_cast<double*>(ws + L.off[17]);
+  r.fock_ws = ws + L.off[18];
+  r.fock_ws_bytes = fws > f2 ? fws : f2;
+  r.red_ws = ws + L.off[19];
+  r.red_ws_bytes = rws;
+  a.hist_E = hist_E ? hist_E : reinterpret_cast<double*>(ws + L.total);
+  a.hist_G = hist_grad ? hist_grad : reinterpret_cast<double*>(ws + L.total) + cf->max_iter;
+  r.nblk = perk_blocks(a.nk);
+
+  const int nb = pb->nb, nb2 = nb * nb;
+  if ((st = set_smem((const void*)k_cg_eig, smem_eig(nb)))) return st;
+  if ((st = set_smem((const void*)k_cg_dir, smem_eig(nb)))) return st;
+  if ((st = set_smem((const void*)k_cg_update, (4 * (size_t)nb2 + nb) * 16 * kSolverWarps))) return st;
+  if ((st = set_smem((const void*)k_cg_grad1, 3 * (size_t)nb2 * 16 * kSolverWarps))) return st;
+
+  if (cf->max_iter > 0) HF_CUDA(cudaMemsetAsync(a.hist_E, 0, sizeof(double) * cf->max_iter, s));
+  if (cf->max_iter > 0) HF_CUDA(cudaMemsetAsync(a.hist_G, 0, sizeof(double) * cf->max_iter, s));
+  // ---- init (solver.py:377-394) ----
+  k_cg_init<<<r.nblk, 256, 0, s>>>(a, static_cast<const double2*>(P0), static_cast<const double*>(pb->w2d),
+                                   pb->weight_sum);
+  HF_LAUNCH_CHECK("k_cg_init");
+  const bool mixed = cf->fp32_exchange != 0;
+  if ((st = cg_fock(r, s, false, nullptr))) return st;
+  k_cg_eig<<<r.nblk, 32 * kSolverWarps, smem_eig(nb), s>>>(a, a.F, 0);
+  HF_LAUNCH_CHECK("k_cg_eig");
+  if ((st = cg_mu(r, s, cf->mu_maxiter, nullptr))) return st;
+
+  // ---- loop (solver.py:603-604), chunks of iterations between host checks ----
+  int host_k = 0, host_active = cf->max_iter > 0;
+  bool fp32 = mixed;
+  int switched_at = -1;
+  const int chunk = cf->chunk > 0 ? cf->chunk : 4;
+  CgScalars hs;
+  while (host_active) {
+    for (int c = 0; c < chunk; ++c)
+      if ((st = cg_iteration(r, s, *cf, fp32))) return st;
+    HF_CUDA(cudaMemcpyAsync(&hs, a.sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, s));
+    HF_CUDA(cudaStreamSynchronize(s));
+    host_k = hs.k;
+    host_active = hs.active;
+    if (!std::isfinite(hs.E)) break;
+    // mixed precision: FP32 exchange until the windowed energy change reaches the FP32
+    // noise floor (or half the iteration budget), then FP64 defect-correction builds
+    // continue from the same state to the requested tolerance.
+    if (fp32 && host_k < cf->max_iter && (!host_active || host_k >= cf->max_iter / 2)) {
+      fp32 = false;
+      switched_at = host_k;
+      k_cg_rearm<<<1, 1, 0, s>>>(a);
+      HF_LAUNCH_CHECK("k_cg_rearm");
+      host_active = 1;
+    }
+  }
+  (void)host_k;
+
+  // ---- finalize (solver.py:613-648) ----
+  k_cg_density<<<r.nblk, 32 * kSolverWarps, (2 * (size_t)nb2 + nb) * 16 * kSolverWarps, s>>>(a, 1);
+  HF_LAUNCH_CHECK("k_cg_density");
+  if ((st = cg_fock(r, s, false, nullptr))) return st;
+  k_cg_eig<<<r.nblk, 32 * kSolverWarps, smem_eig(nb), s>>>(a, a.F, 1);
+  HF_LAUNCH_CHECK("k_cg_eig");
+  if ((st = cg_mu(r, s, cf->mu_maxiter, nullptr))) return st;
+  k_cg_density<<<r.nblk, 32 * kSolverWarps, (2 * (size_t)nb2 + nb) * 16 * kSolverWarps, s>>>(a, 1);
+  HF_LAUNCH_CHECK("k_cg_density");
+  if ((st = cg_fock(r, s, false, nullptr))) return st;
+  if ((st = cg_energy(r, s, &a.sc->E_fin, nullptr))) return st;
+  k_cg_converged<<<1, 1, 0, s>>>(a);
+  HF_LAUNCH_CHECK("k_cg_converged");
+  HF_CUDA(cudaMemcpyAsync(&hs, a.sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, s));
+  HF_CUDA(cudaStreamSynchronize(s));
+  const double out[8] = {hs.mu, hs.E_fin, (double)hs.k, (double)hs.converged, hs.grad_norm,
+                         (double)switched_at, 0.0, 0.0};
+  HF_CUDA(cudaMemcpyAsync(scalars_out, out, sizeof(out), cudaMemcpyHostToDevice, s));
+  HF_CUDA(cudaStreamSynchronize(s));
+  return HF_OK;
+}

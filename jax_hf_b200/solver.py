@@ -1,0 +1,203 @@
+"""Direct-minimisation solver on the GPU (drop-in for jax_hf.solver).
+
+``solve(kernel, P0, n_electrons, config=SolverConfig())`` keeps the reference
+signature and result type (solver.py:240-298, 1098-1251).  With
+``optimizer="cg"`` the whole Riemannian-CG loop runs on the device through
+``hf_cg_solve`` (one C-ABI call per solve); ``optimizer="newton"`` runs the
+trust-region Newton loop of ``newton.py``.
+
+Extensions (keyword-only, default off): ``SolverConfig.fp32_exchange`` turns on
+the mixed-precision mode (FP32 exchange FFT, FP64 defect-correction builds at
+the end); ``SolverConfig.chunk`` is the number of iterations queued between
+host checks of the device stop flag.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import warnings
+from dataclasses import dataclass
+from typing import Any, NamedTuple
+
+import numpy as np
+import torch
+
+from . import _lib
+from .problem import is_marked_zero
+from .utils import validate_electron_count
+
+
+@dataclass(frozen=True)
+class SolverConfig:
+    """solver.py:240-286 (same fields and defaults) + mixed-precision knobs."""
+    max_iter: int = 200
+    tol_E: float = 1e-7
+    tol_grad: float = 0.0
+    denom_scale: float = 1e-3
+    max_step: float = 0.6
+    cg_restart: int = 10
+    bt_shrink: float = 0.5
+    bt_max: int = 8
+    mu_maxiter: int = 25
+    plateau_window: int = 5
+    optimizer: str = "cg"
+    tr_delta0: float = 0.5
+    tr_cg_max: int = 20
+    deflation_targets: Any = None
+    deflation_sigma: float = 0.0
+    deflation_length: float = 1.0
+    block_sizes: tuple | None = None
+    project_fn: Any = None
+    fp32_exchange: bool = False
+    fp32_switch_rel: float = 3e-7
+    chunk: int = 4
+
+
+class SolveResult(NamedTuple):
+    Q: torch.Tensor
+    p: torch.Tensor
+    mu: torch.Tensor
+    density: torch.Tensor
+    fock: torch.Tensor
+    energy: torch.Tensor
+    n_iter: torch.Tensor
+    converged: torch.Tensor
+    history: dict
+
+
+class _CgProblem(C.Structure):
+    _fields_ = [("nk1", C.c_int), ("nk2", C.c_int), ("nb", C.c_int), ("fock_flags", C.c_uint),
+                ("T", C.c_double), ("n_electrons", C.c_double), ("weight_sum", C.c_double),
+                ("h", C.c_void_p), ("VR", C.c_void_p), ("refP", C.c_void_p), ("HH", C.c_void_p),
+                ("w2d", C.c_void_p), ("n_contact", C.c_int), ("contact_g", C.c_void_p),
+                ("contact_Oi", C.c_void_p), ("contact_Oj", C.c_void_p)]
+
+
+class _CgConfig(C.Structure):
+    _fields_ = [("max_iter", C.c_int), ("tol_E", C.c_double), ("tol_grad", C.c_double),
+                ("denom_scale", C.c_double), ("max_step", C.c_double), ("cg_restart", C.c_int),
+                ("bt_shrink", C.c_double), ("bt_max", C.c_int), ("mu_maxiter", C.c_int),
+                ("plateau_window", C.c_int), ("fp32_exchange", C.c_int), ("fp32_switch_rel", C.c_double),
+                ("chunk", C.c_int)]
+
+
+def _bind():
+    L = _lib.lib()
+    if not getattr(L, "_cg_bound", False):
+        L.hf_cg_workspace_size.argtypes = [C.POINTER(_CgProblem), C.POINTER(_CgConfig), C.POINTER(C.c_size_t)]
+        L.hf_cg_workspace_size.restype = C.c_int
+        L.hf_cg_solve.argtypes = [C.c_void_p, C.POINTER(_CgProblem), C.POINTER(_CgConfig), C.c_void_p, C.c_void_p,
+                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.c_void_p, C.c_size_t]
+        L.hf_cg_solve.restype = C.c_int
+        L._cg_bound = True
+    return L
+
+
+class KernelC128:
+    """complex128 views of a kernel's arrays for the device solvers (kept alive with the problem)."""
+
+    def __init__(self, kernel):
+        self.kernel = kernel
+        up = kernel.dtype != torch.complex128
+        cd, rd = torch.complex128, torch.float64
+        self.h = kernel.h.to(cd).contiguous() if up else kernel.h
+        VR = kernel._VR_shifted
+        self.VR = (VR.to(rd) if not VR.is_complex() else VR.to(cd)).contiguous() if up else VR
+        self.refP = None if is_marked_zero(kernel.refP) else kernel.refP.to(cd).contiguous()
+        self.HH = kernel.HH.to(rd).contiguous()
+        self.w2d = kernel.w2d.to(rd).contiguous()
+        self.has_contact = kernel.has_contact
+        self.cg = kernel.contact_g.to(rd).contiguous()
+        self.cOi = kernel.contact_Oi.to(cd).contiguous()
+        self.cOj = kernel.contact_Oj.to(cd).contiguous()
+
+    def flags(self):
+        k = self.kernel
+        f = 0
+        if k.include_exchange:
+            f |= _lib.FOCK_EXCHANGE
+            if not self.VR.is_complex():
+                f |= _lib.FOCK_VR_REAL
+            if tuple(self.VR.shape[-2:]) == (1, 1):
+                f |= _lib.FOCK_VR_SCALAR
+        if k.include_hartree:
+            f |= _lib.FOCK_HARTREE
+        if k.exchange_hermitian_channel_packing:
+            f |= _lib.FOCK_PACKING
+        if self.refP is not None:
+            f |= _lib.FOCK_HAS_REFP
+        return f
+
+    def problem(self, n_electrons):
+        k = self.kernel
+        nk1, nk2, nb = k.shape
+        return _CgProblem(nk1, nk2, nb, self.flags(), float(k.T), float(n_electrons), float(k.weight_sum),
+                          self.h.data_ptr(), self.VR.data_ptr(), _lib.ptr(self.refP), self.HH.data_ptr(),
+                          self.w2d.data_ptr(), int(self.cg.shape[0]) if self.has_contact else 0,
+                          self.cg.data_ptr(), self.cOi.data_ptr(), self.cOj.data_ptr())
+
+
+def _solve_cg(kernel, P0, n_electrons, cfg: SolverConfig, fock_build_fn=None):
+    if cfg.project_fn is not None or cfg.block_sizes is not None or fock_build_fn is not None:
+        from .solver_host import solve_cg_host
+        return solve_cg_host(kernel, P0, n_electrons, cfg, fock_build_fn)
+    L = _bind()
+    dev = kernel.device
+    nk1, nk2, nb = kernel.shape
+    kc = KernelC128(kernel)
+    prob = kc.problem(n_electrons)
+    conf = _CgConfig(int(cfg.max_iter), float(cfg.tol_E), float(cfg.tol_grad), float(cfg.denom_scale),
+                     float(cfg.max_step), int(cfg.cg_restart), float(cfg.bt_shrink), int(cfg.bt_max),
+                     int(cfg.mu_maxiter), int(cfg.plateau_window), int(bool(cfg.fp32_exchange)),
+                     float(cfg.fp32_switch_rel), int(cfg.chunk))
+    need = C.c_size_t(0)
+    _lib.check(L.hf_cg_workspace_size(C.byref(prob), C.byref(conf), C.byref(need)))
+    ws = torch.empty(need.value, dtype=torch.uint8, device=dev)
+    P0t = torch.as_tensor(P0).to(dev, torch.complex128).contiguous() if not (
+        isinstance(P0, torch.Tensor) and P0.dtype == torch.complex128 and P0.device == dev) else P0.contiguous()
+    Q = torch.empty((nk1, nk2, nb, nb), dtype=torch.complex128, device=dev)
+    p = torch.empty((nk1, nk2, nb), dtype=torch.float64, device=dev)
+    P = torch.empty_like(Q)
+    F = torch.empty_like(Q)
+    hE = torch.zeros(max(cfg.max_iter, 1), dtype=torch.float64, device=dev)
+    hG = torch.zeros(max(cfg.max_iter, 1), dtype=torch.float64, device=dev)
+    sc = torch.zeros(8, dtype=torch.float64, device=dev)
+    _lib.check(L.hf_cg_solve(_lib.stream_ptr(dev), C.byref(prob), C.byref(conf), P0t.data_ptr(), Q.data_ptr(),
+                             p.data_ptr(), P.data_ptr(), F.data_ptr(), hE.data_ptr(), hG.data_ptr(), sc.data_ptr(),
+                             ws.data_ptr(), ws.numel()))
+    out_c = kernel.dtype
+    out_r = kernel.real_dtype
+    s = sc.cpu().numpy()
+    hist = dict(E=hE[:cfg.max_iter].to(out_r), grad_norm=hG[:cfg.max_iter].to(out_r))
+    res = SolveResult(Q=Q.to(out_c), p=p.to(out_r), mu=sc[0].to(out_r), density=P.to(out_c), fock=F.to(out_c),
+                      energy=sc[1].clone(), n_iter=torch.tensor(int(s[2]), dtype=torch.int32),
+                      converged=torch.tensor(bool(s[3])), history=hist)
+    res.history["fp32_switch_iter"] = int(s[5])
+    return res
+
+
+def solve_direct_minimization(kernel, P0, n_electrons: float, *, config: SolverConfig | None = None,
+                              fock_build_fn=None) -> SolveResult:
+    """Direct-minimisation HF solver (solver.py:1098-1247)."""
+    if config is None:
+        config = SolverConfig()
+    validate_electron_count(kernel.w2d, kernel.h.shape[-1], n_electrons, context="n_electrons")
+    optimizer = str(config.optimizer).lower()
+    if optimizer not in ("cg", "newton"):
+        raise ValueError(f"Unknown optimizer {config.optimizer!r}; expected 'cg' or 'newton'.")
+    deflation_on = config.deflation_targets is not None and float(config.deflation_sigma) > 0.0
+    if deflation_on and optimizer != "newton":
+        raise ValueError("deflation is only supported with optimizer='newton' "
+                         f"(got optimizer={config.optimizer!r}).")
+    if optimizer == "newton":
+        if kernel.real_dtype != torch.float64:
+            warnings.warn(
+                "optimizer='newton' needs float64 precision to converge reliably; the kernel is float32. "
+                "Build the kernel in complex128. The CG optimizer works in float32.", stacklevel=2)
+        from .newton import solve_newton
+        return solve_newton(kernel, P0, n_electrons, config, fock_build_fn)
+    return _solve_cg(kernel, P0, n_electrons, config, fock_build_fn)
+
+
+solve = solve_direct_minimization
