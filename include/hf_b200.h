@@ -72,6 +72,7 @@ int hf_fock_build(void* stream, int dtype, unsigned flags, int nk1, int nk2, int
                   const void* contact_Oi, const void* contact_Oj, void* Sigma, void* H, void* F,
                   void* workspace, size_t workspace_bytes);
 
+
 /* ---- Objective reductions (compensated, FP64 accumulation) -----------------
  * hf_energy replaces fock.hf_energy (fock.py:100-111):
  *   E = sum_k w_k Re Tr[(h + (Sigma + H)/2) P]

@@ -53,6 +53,8 @@ _SIGS = {
     "hf_cayley_unitary": ([vp, i32, i32, i32, vp, vp, f64, vp], i32),
     "hf_diag_UFU": ([vp, i32, i32, i32, vp, vp, vp, f64, vp], i32),
     "hf_qr_retract": ([vp, i32, i32, i32, vp, f64, vp], i32),
+    "hf_cg_workspace_size": ([vp, vp, psz], i32),
+    "hf_cg_solve": ([vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, sz], i32),
 }
 
 

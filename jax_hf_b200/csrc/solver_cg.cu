@@ -705,6 +705,7 @@ extern "C" int hf_cg_solve(void* stream, const hf_cg_problem* pb, const hf_cg_co
   if ((st = set_smem((const void*)k_cg_update, (4 * (size_t)nb2 + nb) * 16 * kSolverWarps))) return st;
   if ((st = set_smem((const void*)k_cg_grad1, 3 * (size_t)nb2 * 16 * kSolverWarps))) return st;
 
+  HF_CUDA(cudaMemsetAsync(r.H, 0, sizeof(double2) * nb2, s));  // H stays zero without Hartree
   if (cf->max_iter > 0) HF_CUDA(cudaMemsetAsync(a.hist_E, 0, sizeof(double) * cf->max_iter, s));
   if (cf->max_iter > 0) HF_CUDA(cudaMemsetAsync(a.hist_G, 0, sizeof(double) * cf->max_iter, s));
   // ---- init (solver.py:377-394) ----

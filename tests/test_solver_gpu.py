@@ -1,0 +1,117 @@
+"""GPU parity of the device-resident CG solver against the CPU oracle (solver.py:307-660).
+
+Both run the same FP64 algorithm from the same start, so iteration counts agree
+to within a couple of steps and the converged energies to round-off of the
+stopping point; invariants follow tests/test_solver.py of the reference.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import hf_oracle as O
+from jax_hf_b200 import synthetic as S
+
+pytestmark = pytest.mark.gpu
+
+
+def _two_band(nk=1, T=0.2, ex=0.25):
+    h = np.zeros((nk, nk, 2, 2), complex)
+    h[..., 0, 0] = -0.5
+    h[..., 1, 1] = 0.5
+    return dict(weights=np.ones((nk, nk)), hamiltonian=h, coulomb_q=np.full((nk, nk, 1, 1), ex), T=T)
+
+
+def _dirac(nk=4, m=0.3, v=1.0, T=0.1, ex=0.7):
+    ks = (np.arange(nk) - nk // 2) * (2 * np.pi / nk)
+    KX, KY = np.meshgrid(ks, ks, indexing="ij")
+    h = np.zeros((nk, nk, 2, 2), complex)
+    h[..., 0, 0] = m
+    h[..., 1, 1] = -m
+    h[..., 0, 1] = v * (KX - 1j * KY)
+    h[..., 1, 0] = v * (KX + 1j * KY)
+    return dict(weights=np.ones((nk, nk)), hamiltonian=h, coulomb_q=np.full((nk, nk, 1, 1), ex), T=T)
+
+
+def _fourier(nk, nb, V, T, seed):
+    p = S.fourier_problem(nk, nb, 2.0, seed, V=V, T=T)
+    return dict(weights=p.weights, hamiltonian=p.hamiltonian, coulomb_q=p.coulomb_q, T=T)
+
+
+def _contact(nk=2, T=0.05):
+    h = np.zeros((nk, nk, 2, 2), complex)
+    h[..., 0, 0] = -1.0
+    h[..., 1, 1] = 1.0
+    for i in range(nk):
+        for j in range(nk):
+            h[i, j, 0, 1] = h[i, j, 1, 0] = 0.4 + 0.1 * (i + j)
+    sz = np.diag([1.0, -1.0]).astype(complex)
+    return dict(weights=np.ones((nk, nk)), hamiltonian=h, coulomb_q=np.full((nk, nk, 1, 1), 0.1), T=T,
+                contact_terms=[(0.3, sz, sz)])
+
+
+CASES = [
+    ("two_band_k1", _two_band(), 1.0, dict(max_iter=100, tol_E=1e-8)),
+    ("two_band_k2", _two_band(nk=2, T=0.1), 4.0, dict(max_iter=100, tol_E=1e-7)),
+    ("dirac_k4", _dirac(), 16.0, dict(max_iter=200, tol_E=1e-9)),
+    ("fourier_12_nb4_scalar", _fourier(12, 4, "scalar", 0.1, 3), 2.0, dict(max_iter=200, tol_E=1e-10)),
+    ("fourier_10_nb3_layer", _fourier(10, 3, "layer", 0.05, 4), 1.3, dict(max_iter=200, tol_E=1e-10)),
+    ("contact_k2", _contact(), 4.0, dict(max_iter=200, tol_E=1e-10)),
+    ("gradstop_dirac_k4", _dirac(), 16.0, dict(max_iter=300, tol_grad=1e-6)),
+]
+
+
+def _run_pair(kw, ne, cfg):
+    import jax_hf_b200 as G
+    from jax_hf_b200.solver import SolverConfig, solve
+    K = G.HartreeFockKernel(**kw)
+    Ko = O.Kernel(**kw)
+    P0 = np.zeros_like(np.asarray(kw["hamiltonian"], complex))
+    r = solve(K, torch.as_tensor(P0, device="cuda"), ne, config=SolverConfig(**cfg))
+    ro = O.solve(Ko, P0, ne, config=O.SolverConfig(**cfg))
+    return K, Ko, r, ro
+
+
+@pytest.mark.parametrize("name,kw,ne,cfg", CASES, ids=[c[0] for c in CASES])
+def test_cg_matches_oracle(cuda, name, kw, ne, cfg):
+    K, Ko, r, ro = _run_pair(kw, ne, cfg)
+    E, Eo = float(r.energy), ro["energy"]
+    assert bool(r.converged) == ro["converged"]
+    assert abs(int(r.n_iter) - ro["n_iter"]) <= 2
+    assert abs(E - Eo) <= max(1e-9 * abs(Eo), 50 * cfg.get("tol_E", 1e-9))
+    D = r.density.cpu().numpy()
+    assert np.abs(D - ro["density"]).max() < 1e-4
+    assert abs(float(r.mu) - ro["mu"]) < 1e-4
+    # reference invariants (tests/test_solver.py:50-97)
+    np.testing.assert_allclose(D, np.conj(np.swapaxes(D, -1, -2)), atol=1e-12)
+    w2d = K.w2d.cpu().numpy()
+    n_tot = float(np.sum(w2d[..., None] * r.p.cpu().numpy()))
+    assert abs(n_tot - ne) < 1e-6 * max(1.0, ne)
+    n = int(r.n_iter)
+    assert np.all(np.isfinite(r.history["E"][:n].cpu().numpy()))
+    F = r.fock.cpu().numpy()
+    comm = F @ D - D @ F
+    rms = np.sqrt(np.sum(w2d * np.sum(np.abs(comm) ** 2, axis=(-2, -1))) / np.sum(w2d))
+    assert rms < 1e-3
+
+
+def test_cg_mixed_precision_energy(cuda):
+    """FP32 exchange + FP64 defect correction reaches the FP64 energy within 1e-9 relative."""
+    import jax_hf_b200 as G
+    from jax_hf_b200.solver import SolverConfig, solve
+    kw = _fourier(24, 4, "layer", 0.1, 6)
+    K = G.HartreeFockKernel(**kw)
+    P0 = torch.zeros((24, 24, 4, 4), dtype=torch.complex128, device="cuda")
+    r64 = solve(K, P0, 2.0, config=SolverConfig(max_iter=300, tol_E=1e-11))
+    rmx = solve(K, P0, 2.0, config=SolverConfig(max_iter=300, tol_E=1e-11, fp32_exchange=True))
+    E64, Emx = float(r64.energy), float(rmx.energy)
+    assert abs(Emx - E64) <= 1e-9 * abs(E64)
+    assert rmx.history["fp32_switch_iter"] >= 0
+
+
+def test_cg_rejects_unreachable_count(cuda):
+    import jax_hf_b200 as G
+    from jax_hf_b200.solver import solve
+    K = G.HartreeFockKernel(**_two_band())
+    with pytest.raises(ValueError, match="physically reachable range"):
+        solve(K, torch.zeros((1, 1, 2, 2), dtype=torch.complex128, device="cuda"), 3.0)
