@@ -72,6 +72,25 @@ int hf_fock_build(void* stream, int dtype, unsigned flags, int nk1, int nk2, int
                   const void* contact_Oi, const void* contact_Oj, void* Sigma, void* H, void* F,
                   void* workspace, size_t workspace_bytes);
 
+/* Same Fock build as hf_fock_build, for callers that cannot allocate device
+ * memory (a framework custom-call handler that owns all device buffers, code
+ * running under CUDA stream capture): the scratch is a library-owned static
+ * device array of HF_FOCK_STATIC_SCRATCH_BYTES, so no workspace argument.
+ * No counterpart in the reference (jax_hf allocates through XLA).
+ *  - Returns HF_ERR_WORKSPACE if the mesh needs more scratch than the array
+ *    holds (hf_fock_workspace_size() > HF_FOCK_STATIC_SCRATCH_BYTES; e.g. up
+ *    to 192x192 with nb = 8 in complex128).
+ *  - The first call on a device looks up the array's device address; make it
+ *    before any stream capture.  The array stays allocated on every device
+ *    that loaded this part of the library until the process exits.
+ *  - All calls on a device share the array: calls that may overlap on the GPU
+ *    race and must be serialised by the caller. */
+#define HF_FOCK_STATIC_SCRATCH_BYTES (40u << 20)
+int hf_fock_build_static_scratch(void* stream, int dtype, unsigned flags, int nk1, int nk2, int nb,
+                                 const void* P, const void* h, const void* VR, const void* refP,
+                                 const void* HH, const void* w2d, int n_contact, const void* contact_g,
+                                 const void* contact_Oi, const void* contact_Oj, void* Sigma, void* H,
+                                 void* F);
 
 /* ---- Objective reductions (compensated, FP64 accumulation) -----------------
  * hf_energy replaces fock.hf_energy (fock.py:100-111):

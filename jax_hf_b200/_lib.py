@@ -40,6 +40,8 @@ _SIGS = {
     "hf_fock_workspace_size": ([i32, u32, i32, i32, i32, psz], i32),
     "hf_fock_build": ([vp, i32, u32, i32, i32, i32, vp, vp, vp, vp, vp, vp, i32, vp, vp, vp,
                        vp, vp, vp, vp, sz], i32),
+    "hf_fock_build_static_scratch": ([vp, i32, u32, i32, i32, i32, vp, vp, vp, vp, vp, vp, i32, vp, vp, vp,
+                                      vp, vp, vp], i32),
     "hf_reduce_workspace_size": ([i32, i32, i32, psz], i32),
     "hf_energy": ([vp, i32, i32, i32, i32, vp, vp, vp, vp, i32, vp, vp, vp, sz], i32),
     "hf_occupation_entropy": ([vp, i32, i32, i32, i32, vp, vp, vp, vp, sz], i32),

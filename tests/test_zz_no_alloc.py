@@ -1,0 +1,96 @@
+"""hf_fock_build_static_scratch: the Fock build for callers that cannot allocate.
+
+Some callers cannot hand the library a workspace: a framework custom-call
+handler whose framework owns all device memory, or code running under CUDA
+stream capture, where cudaMalloc is refused or synchronises the device.  For
+them the library offers a Fock build whose scratch is a fixed static device
+array.  This test calls it through the C ABI and checks that two calls in a
+row give the same Sigma, H and F as hf_fock_build with a caller workspace
+(relative tolerance 1e-12, as for every complex128 parity test), and that a
+mesh larger than the array is refused with an error instead of running.
+
+The file is named so that pytest collects it last; it also passes when run on
+its own in a fresh process.
+"""
+
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+from jax_hf_b200 import synthetic as S
+
+pytestmark = pytest.mark.gpu
+
+
+def _inputs(seed):
+    rng = np.random.default_rng(seed)
+    nk1, nk2, nb = 48, 40, 6
+    prob = S.fourier_problem(48, nb, 2.0, seed, V="layer")
+    h = np.ascontiguousarray(prob.hamiltonian[:nk1, :nk2])
+    Vq = np.ascontiguousarray(prob.coulomb_q[:nk1, :nk2])
+    w = np.full((nk1, nk2), 1.0 / (nk1 * nk2))
+    P = np.ascontiguousarray(S.haar_density(48, nb, seed + 3)[:nk1, :nk2])
+    refP = 0.5 * np.ascontiguousarray(S.haar_density(48, nb, seed + 4)[:nk1, :nk2])
+    HH = rng.normal(size=(nb, nb))
+    Oa = rng.normal(size=(nb, nb)) + 1j * rng.normal(size=(nb, nb))
+    return dict(h=h, Vq=Vq, w=w, P=P, refP=refP, HH=HH + HH.T, Oa=Oa, nb=nb)
+
+
+def _call_both(d):
+    import jax_hf_b200 as G
+    from jax_hf_b200 import _lib
+
+    L = _lib.lib()
+    K = G.HartreeFockKernel(d["w"], d["h"], d["Vq"], 0.1, include_hartree=True, reference_density=d["refP"],
+                            hartree_matrix=d["HH"], contact_terms=[(0.25, d["Oa"], d["Oa"].conj().T)])
+    nk1, nk2, nb = K.shape
+    flags = _lib.FOCK_EXCHANGE | _lib.FOCK_HARTREE | _lib.FOCK_HAS_REFP
+    VR = K._VR_shifted
+    if not VR.is_complex():
+        flags |= _lib.FOCK_VR_REAL
+    P = torch.as_tensor(d["P"], device="cuda")
+    args = (P.data_ptr(), K.h.data_ptr(), VR.data_ptr(), K.refP.data_ptr(), K.HH.data_ptr(), K.w2d.data_ptr(),
+            1, K.contact_g.data_ptr(), K.contact_Oi.data_ptr(), K.contact_Oj.data_ptr())
+    stream = torch.cuda.current_stream().cuda_stream
+    ref = [torch.empty_like(P), torch.empty((nb, nb), dtype=P.dtype, device="cuda"), torch.empty_like(P)]
+    need = C.c_size_t(0)
+    _lib.check(L.hf_fock_workspace_size(_lib.HF_C128, flags, nk1, nk2, nb, C.byref(need)))
+    ws = torch.empty(need.value, dtype=torch.uint8, device="cuda")
+    _lib.check(L.hf_fock_build(stream, _lib.HF_C128, flags, nk1, nk2, nb, *args, ref[0].data_ptr(),
+                               ref[1].data_ptr(), ref[2].data_ptr(), ws.data_ptr(), ws.numel()))
+    out = [torch.full_like(ref[0], float("nan")), torch.full_like(ref[1], float("nan")),
+           torch.full_like(ref[2], float("nan"))]
+    _lib.check(L.hf_fock_build_static_scratch(stream, _lib.HF_C128, flags, nk1, nk2, nb, *args, out[0].data_ptr(),
+                                              out[1].data_ptr(), out[2].data_ptr()))
+    torch.cuda.synchronize()
+    return ref, out
+
+
+def _rel(a, b):
+    return float((a - b).abs().max() / b.abs().max().clamp_min(1e-300))
+
+
+def test_static_scratch_matches_workspace_build_twice(cuda):
+    for seed in (21, 22):   # two calls in a row, different inputs: no state leaks between calls
+        ref, out = _call_both(_inputs(seed))
+        for r, o in zip(ref, out):
+            assert torch.isfinite(o).all()
+            assert _rel(o, r) <= 1e-12
+
+
+def test_static_scratch_rejects_oversized_mesh(cuda):
+    from jax_hf_b200 import _lib
+
+    L = _lib.lib()
+    flags = _lib.FOCK_EXCHANGE | _lib.FOCK_VR_REAL
+    need = C.c_size_t(0)
+    _lib.check(L.hf_fock_workspace_size(_lib.HF_C128, flags, 256, 256, 8, C.byref(need)))
+    assert need.value > (40 << 20)
+    dummy = torch.zeros(1, dtype=torch.complex128, device="cuda")
+    p = dummy.data_ptr()
+    st = L.hf_fock_build_static_scratch(torch.cuda.current_stream().cuda_stream, _lib.HF_C128, flags, 256, 256, 8,
+                                        p, p, p, None, None, p, 0, None, None, None, p, None, p)
+    assert st == _lib.HF_ERR_WORKSPACE
+    assert b"static array" in L.hf_last_error()
