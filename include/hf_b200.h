@@ -47,6 +47,7 @@ extern "C" {
 #define HF_FOCK_VR_REAL (1u << 4)   /* VR is stored as a real array                    */
 #define HF_FOCK_FFT_FP32 (1u << 5)  /* complex128 storage, exchange FFT in FP32        */
 #define HF_FOCK_HAS_REFP (1u << 6)  /* refP is non-zero and must be subtracted         */
+#define HF_FOCK_GENERIC_FFT (1u << 7) /* force the generic shared-memory FFT engine    */
 
 const char* hf_last_error(void);
 const char* hf_status_string(int status);
@@ -152,11 +153,64 @@ int hf_diag_UFU(void* stream, int dtype, int batch, int nb, const void* V, const
 int hf_qr_retract(void* stream, int dtype, int batch, int nb, const void* G, double tau,
                   void* U);
 
+/* ---- Solver building blocks (complex128 / float64) ----------------------------
+ * Used by the SCF loop (reference_scf.py:222-365) and the trust-region Newton
+ * loop (solver.py:686-1078).  Reductions write float64 results to device
+ * memory; `ws` is scratch of hf_ops_workspace_size() bytes.
+ *  hf_fermi          mode 0: fermidirac(eps-mu, T) (utils.py:51-53); mode 1: sigmoid((mu-eps)/max(T,1e-12))
+ *                    (solver.py:394); mode 2: eps + shift (1 - fermidirac(eps-mu, T)) (reference_scf.py:92).
+ *                    mu is a device scalar.
+ *  hf_scf_residuals  comm = F P - P F, delta = Pn - P and sums3 = {sum w|delta|^2, sum w|comm|^2,
+ *                    sum w Re tr(F delta)}  (reference_scf.py:291-295, 319-320)
+ *  hf_gram           DIIS B_ij = sum_k w Re tr(R_i^H R_j), upper triangle row-major (reference_scf.py:110-111)
+ *  hf_lincomb        out = sum_i c_i X_i, c on device (reference_scf.py:305)
+ *  hf_axpby          out = [herm](a x + b y); hf_axpby_real the same for real vectors
+ *  hf_jdot           sum_k wX sum Re(conj(aX) bX) + sum_k wp sum ap bp (solver.py:205-233, 783-787)
+ *  hf_orbital_grad   G = skew((p_j - p_i) Ft) offdiag, eps = Re diag Ft (solver.py:898-900)
+ *  hf_newton_prec    z = (rX / sqrt(gap^2 + lam^2), rp p(1-p)/T) + sum w2d zp (solver.py:907-913)
+ *  hf_sub_scalar     x -= scale * c[0]   (particle-number projection, solver.py:224-233)
+ *  hf_newton_dP      dP = herm(Q (X o dpij + diag dp) Q^H) (solver.py:917-919)
+ *  hf_newton_hvp     HX, Hp of the joint Hessian from Fr = F[dP] (solver.py:920-930)
+ *  hf_matmul, hf_real_diag  per-k C = A B, d = Re diag A
+ */
+int hf_ops_workspace_size(size_t* bytes);
+int hf_fermi(void* stream, size_t n, const double* eps, const double* mu, double T, int mode, double shift,
+             double* out);
+int hf_scf_residuals(void* stream, int nk, int nb, const void* F, const void* P, const void* Pn, const double* w,
+                     void* comm, void* delta, double* sums3, void* ws);
+int hf_gram(void* stream, int n, size_t stride, int nk, int nb, const void* R, const double* w, double* B_out,
+            void* ws);
+int hf_lincomb(void* stream, int n, size_t stride, size_t len, const void* X, const double* c, void* out);
+int hf_axpby(void* stream, size_t nk, int nb, double a, const void* x, double b, const void* y, int herm,
+             void* out);
+int hf_axpby_real(void* stream, size_t n, double a, const double* x, double b, const double* y, double* out);
+int hf_jdot(void* stream, size_t nk, int nb, const void* aX, const void* bX, const double* wX, const double* ap,
+            const double* bp, const double* wp, double* out, void* ws);
+int hf_orbital_grad(void* stream, size_t nk, int nb, const void* Ft, const double* p, void* G, double* eps);
+int hf_newton_prec(void* stream, size_t nk, int nb, const void* rX, const double* rp, const double* eps,
+                   const double* p, double lam, double T, double clipv, const double* w2d, void* zX, double* zp,
+                   double* wsum_out, void* ws);
+int hf_sub_scalar(void* stream, size_t n, double* x, const double* c, double scale);
+int hf_newton_dP(void* stream, int nk, int nb, const void* Q, const void* X, const double* dp, const double* p,
+                 void* dP);
+int hf_newton_hvp(void* stream, int nk, int nb, const void* Q, const void* Ft, const void* X, const double* dp,
+                  const double* p, const void* Fr, const void* h, double T, double clipv, double pen,
+                  const void* dPpen, void* HX, double* Hp, const double* w2d, double* wsum_out, void* ws);
+int hf_matmul(void* stream, int nk, int nb, const void* A, const void* B, void* C);
+int hf_real_diag(void* stream, size_t nk, int nb, const void* A, double* d);
+
 /* ---- Device-resident solvers ---------------------------------------------------
  * The problem is a HartreeFockKernel's arrays (problem.py:201-217 as_args) in
  * complex128 storage.  fock_flags carries HF_FOCK_EXCHANGE/HARTREE/PACKING/
  * VR_SCALAR/VR_REAL/HAS_REFP exactly as for hf_fock_build.
  */
+/* Optional host callbacks of the CG driver, invoked when an iteration is
+ * enqueued (they must enqueue their device work on `stream` and return an
+ * hf status): fock_cb replaces the built-in Fock build (Sigma, H (nb x nb), F
+ * from P), project_cb maps P -> herm(project(P)) in place. */
+typedef int (*hf_fock_callback)(void* user, void* stream, const void* P, void* Sigma, void* H, void* F);
+typedef int (*hf_project_callback)(void* user, void* stream, void* P);
+
 typedef struct hf_cg_problem {
   int nk1, nk2, nb;
   unsigned fock_flags;
@@ -170,6 +224,8 @@ typedef struct hf_cg_problem {
   const void* contact_g;  /* (t,) float64                                   */
   const void* contact_Oi; /* (t, nb, nb) complex128                         */
   const void* contact_Oj;
+  void* sigma_buf;        /* optional caller buffer for Sigma (nk1, nk2, nb, nb) */
+  void* h_buf;            /* optional caller buffer for H (nb, nb)               */
 } hf_cg_problem;
 
 /* SolverConfig fields (solver.py:240-286) plus the mixed-precision policy:
@@ -186,6 +242,9 @@ typedef struct hf_cg_config {
   int fp32_exchange;
   double fp32_switch_rel;
   int chunk;
+  hf_fock_callback fock_cb;       /* NULL: built-in hf_fock_build */
+  hf_project_callback project_cb; /* NULL: no projection           */
+  void* cb_user;
 } hf_cg_config;
 
 /* Direct-minimisation CG (solver.py:307-660, optimizer="cg"): replaces

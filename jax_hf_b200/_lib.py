@@ -28,6 +28,7 @@ FOCK_VR_SCALAR = 1 << 3
 FOCK_VR_REAL = 1 << 4
 FOCK_FFT_FP32 = 1 << 5
 FOCK_HAS_REFP = 1 << 6
+FOCK_GENERIC_FFT = 1 << 7
 
 vp, i32, u32, f64, sz = C.c_void_p, C.c_int, C.c_uint, C.c_double, C.c_size_t
 pf64 = C.POINTER(C.c_double)
@@ -55,6 +56,21 @@ _SIGS = {
     "hf_cayley_unitary": ([vp, i32, i32, i32, vp, vp, f64, vp], i32),
     "hf_diag_UFU": ([vp, i32, i32, i32, vp, vp, vp, f64, vp], i32),
     "hf_qr_retract": ([vp, i32, i32, i32, vp, f64, vp], i32),
+    "hf_ops_workspace_size": ([psz], i32),
+    "hf_fermi": ([vp, sz, vp, vp, f64, i32, f64, vp], i32),
+    "hf_scf_residuals": ([vp, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp], i32),
+    "hf_gram": ([vp, i32, sz, i32, i32, vp, vp, vp, vp], i32),
+    "hf_lincomb": ([vp, i32, sz, sz, vp, vp, vp], i32),
+    "hf_axpby": ([vp, sz, i32, f64, vp, f64, vp, i32, vp], i32),
+    "hf_axpby_real": ([vp, sz, f64, vp, f64, vp, vp], i32),
+    "hf_jdot": ([vp, sz, i32, vp, vp, vp, vp, vp, vp, vp, vp], i32),
+    "hf_orbital_grad": ([vp, sz, i32, vp, vp, vp, vp], i32),
+    "hf_newton_prec": ([vp, sz, i32, vp, vp, vp, vp, f64, f64, f64, vp, vp, vp, vp, vp], i32),
+    "hf_sub_scalar": ([vp, sz, vp, vp, f64], i32),
+    "hf_newton_dP": ([vp, i32, i32, vp, vp, vp, vp, vp], i32),
+    "hf_newton_hvp": ([vp, i32, i32, vp, vp, vp, vp, vp, vp, vp, f64, f64, f64, vp, vp, vp, vp, vp, vp], i32),
+    "hf_matmul": ([vp, i32, i32, vp, vp, vp], i32),
+    "hf_real_diag": ([vp, sz, i32, vp, vp], i32),
     "hf_cg_workspace_size": ([vp, vp, psz], i32),
     "hf_cg_solve": ([vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, sz], i32),
 }

@@ -22,39 +22,9 @@
 
 #include "common.cuh"
 #include "fft_engine.cuh"
+#include "fock_params.cuh"
 
 namespace hf {
-
-constexpr int kMaxNb = 32;
-constexpr int kMaxSlotTable = 1280;
-constexpr int kThreads = 256;
-
-struct FockParams {
-  int nk1, nk2, nb, nb2, LS, ngroups;
-  unsigned flags;
-  int n_contact;
-  double scale;  // -1 / (nk1 nk2)
-  FftPlan1D row, col;
-  const void* P;
-  const void* h;
-  const void* VR;
-  const void* refP;
-  const void* w2d;
-  const void* HH;
-  const void* cg;
-  const void* cOi;
-  const void* cOj;
-  void* Sigma;
-  void* F;
-  void* Hout;
-  void* scratch;
-  double2* rho_part;  // [nk1][ngroups*LS]
-  double2* sigc;      // [nb*nb] contact sigma
-  double* hdiag;      // [nb] Hartree diagonal
-  const int* active;  // optional device flag: kernels return at once when *active == 0
-  int16_t chan[kMaxSlotTable];
-  int16_t partner[kMaxSlotTable];
-};
 
 // ------------------------------------------------------------ planning -----
 struct SlotPlan {
@@ -129,14 +99,14 @@ static size_t fock_smem_bytes(int n, int LS) {
   return (size_t)(2 * n * LS + n) * sizeof(cpx_t<FT>);
 }
 
-static int plan_slots(int nb, bool packing, int nmax, size_t celem, SlotPlan& out) {
+static int plan_slots(int nb, bool packing, int nmax, size_t celem, int max_ls, SlotPlan& out) {
   auto units = make_units(nb, packing);
   int maxu = 0, total = 0;
   for (auto& u : units) { maxu = std::max<int>(maxu, (int)u.size()); total += (int)u.size(); }
   const size_t kTwoPerSm = 113 * 1024, kOnePerSm = 227 * 1024;
   int best = -1, best_pad = 1 << 30, best_fit2 = 0;
   std::vector<std::vector<int>> groups, best_groups;
-  for (int LS = maxu; LS <= 32; ++LS) {
+  for (int LS = maxu; LS <= max_ls; ++LS) {
     if (!pack_units(units, LS, groups)) continue;
     size_t smem = (size_t)(2 * nmax * LS + nmax) * celem;
     if (smem > kOnePerSm) continue;
@@ -452,7 +422,8 @@ static size_t fft_elem(int dtype, unsigned flags) {
 
 static int get_plan(int dtype, unsigned flags, int nk1, int nk2, int nb, SlotPlan& sp) {
   const bool packing = (flags & HF_FOCK_PACKING) != 0;
-  int st = plan_slots(nb, packing, std::max(nk1, nk2), fft_elem(dtype, flags), sp);
+  const int max_ls = (fast_length(nk1) && fast_length(nk2)) ? 16 : 32;
+  int st = plan_slots(nb, packing, std::max(nk1, nk2), fft_elem(dtype, flags), max_ls, sp);
   if (st != HF_OK) return fail(st, "mesh too large for the shared-memory FFT (nk1, nk2 <= 768 in complex128)");
   return HF_OK;
 }
@@ -471,6 +442,11 @@ static int launch_fock(FockParams& p, cudaStream_t stream, bool need_consts) {
     HF_LAUNCH_CHECK("k_fock_rho_part");
     k_fock_consts<ST><<<1, 256, 0, stream>>>(p);
     HF_LAUNCH_CHECK("k_fock_consts");
+  }
+  if (!(p.flags & HF_FOCK_GENERIC_FFT)) {
+    bool handled = false;
+    const int st = fast_fock<ST, FT>(p, stream, &handled);
+    if (st != HF_OK || handled) return st;
   }
   if (exch) {
     k_fock_row_fwd<ST, FT><<<grow, kThreads, sm_row, stream>>>(p);

@@ -1,0 +1,392 @@
+// Fast Fock-build passes for compile-time mesh lengths (see fft_reg.cuh).
+//
+// Thread layout of every pass: 16 slot lanes x TPL line parts; lane s of a
+// half-warp owns band-pair slot s of the group, part t = threadIdx.x / 16.
+// Global loads/stores go straight between HBM/L2 and registers: for a fixed
+// element index the 16 lanes touch 16 consecutive slots (scratch) or one
+// k-point's channel tiles (P, h, Sigma, F), so every access is a few whole
+// 32-byte sectors.  Streamed operands use cache-streaming hints (__ldcs /
+// __stcs) so that the spectrum scratch, which is re-read by the next pass,
+// keeps its place in L2.
+//   row_fwd : P - refP (pattern A along k2) -> FFT -> scratch (pattern B)
+//   col     : scratch column (pattern A along k1) -> FFT -> x(-VR/N) -> IFFT -> scratch
+//   row_inv : scratch (pattern B) -> IFFT -> epilogue (contact, Hartree, herm via a
+//             lane shuffle with the transposed channel, + h) -> Sigma, F
+#pragma once
+
+#include "fft_reg.cuh"
+#include "fock_params.cuh"
+
+namespace hf {
+
+template <typename C>
+__device__ __forceinline__ C ld_stream(const C* p) { return __ldcs(p); }
+template <typename C>
+__device__ __forceinline__ void st_stream(C* p, C v) { __stcs(p, v); }
+
+// cp.async helpers: 16/8-byte global->shared copies that bypass registers.
+// src_bytes = 0 zero-fills the destination (padding slots).
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
+               "r"(valid ? 16 : 0));
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src, bool valid) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
+               "r"(valid ? 8 : 0));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Each fast pass is a persistent kernel: CTA b handles items b, b + grid, ...
+// (item = slot group g + ngroups * line), and while it transforms one item the
+// copies of the next one are already in flight into `stage`.  Every thread
+// copies exactly the elements it later reads, so completion needs no barrier.
+
+// Stages the pattern-A elements of row k1 (P - refP along k2) for one thread.
+template <typename ST, typename FT, class S>
+__device__ __forceinline__ void stage_row_fwd(const FockParams& p, cpx_t<FT>* stage, int k1, int c, int t, int s) {
+  using SC = cpx_t<ST>;
+  const SC* P = static_cast<const SC*>(p.P) + (size_t)k1 * S::N * p.nb2 + (c < 0 ? 0 : c);
+  if constexpr (sizeof(SC) == sizeof(cpx_t<FT>)) {
+#pragma unroll
+    for (int i = 0; i < S::E1; ++i)
+#pragma unroll
+      for (int n1 = 0; n1 < S::N1; ++n1) {
+        const int n = S::idxA(t, i, n1);
+        if constexpr (sizeof(SC) == 16) cp_async16(stage + n * 16 + s, P + (size_t)n * p.nb2, c >= 0);
+        else cp_async8(stage + n * 16 + s, P + (size_t)n * p.nb2, c >= 0);
+      }
+  }
+  cp_async_commit();
+}
+
+template <typename ST, typename FT, class S>
+__global__ void __launch_bounds__(16 * S::TPL) k_fast_row_fwd(const __grid_constant__ FockParams p) {
+  if (p.active && !*p.active) return;
+  using SC = cpx_t<ST>;
+  using FC = cpx_t<FT>;
+  constexpr bool kStage = sizeof(SC) == sizeof(FC);  // mixed precision converts in registers
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  FC* tw = reinterpret_cast<FC*>(smem_raw);
+  FC* buf = tw + S::N;
+  FC* stage = buf + 16 * S::N;
+  const int t = threadIdx.x >> 4, s = threadIdx.x & 15, LS = p.LS;
+  const int nitems = p.ngroups * p.nk1;
+  build_twiddles<FT>(tw, S::N);
+  const bool has_ref = (p.flags & HF_FOCK_HAS_REFP) != 0;
+  int item = blockIdx.x;
+  if (kStage && item < nitems) {
+    const int g = item % p.ngroups;
+    stage_row_fwd<ST, FT, S>(p, stage, item / p.ngroups, s < LS ? p.chan[g * LS + s] : -1, t, s);
+  }
+  __syncthreads();
+  for (; item < nitems; item += gridDim.x) {
+    const int g = item % p.ngroups, k1 = item / p.ngroups;
+    const int c = s < LS ? p.chan[g * LS + s] : -1;
+    FC x[S::E];
+    if constexpr (kStage) {
+      cp_async_wait_all();
+#pragma unroll
+      for (int i = 0; i < S::E1; ++i)
+#pragma unroll
+        for (int n1 = 0; n1 < S::N1; ++n1) x[i * S::N1 + n1] = stage[S::idxA(t, i, n1) * 16 + s];
+      const int nx = item + gridDim.x;
+      if (nx < nitems) {
+        const int g2 = nx % p.ngroups;
+        stage_row_fwd<ST, FT, S>(p, stage, nx / p.ngroups, s < LS ? p.chan[g2 * LS + s] : -1, t, s);
+      }
+    } else {
+      const SC* P = static_cast<const SC*>(p.P) + (size_t)k1 * S::N * p.nb2 + (c < 0 ? 0 : c);
+#pragma unroll
+      for (int i = 0; i < S::E1; ++i)
+#pragma unroll
+        for (int n1 = 0; n1 < S::N1; ++n1)
+          x[i * S::N1 + n1] = c >= 0 ? cvt<FC>(ld_stream(P + (size_t)S::idxA(t, i, n1) * p.nb2)) : mk<FC>(0.0, 0.0);
+    }
+    if (has_ref && c >= 0) {
+      const SC* R = static_cast<const SC*>(p.refP) + (size_t)k1 * S::N * p.nb2 + c;
+#pragma unroll
+      for (int i = 0; i < S::E1; ++i)
+#pragma unroll
+        for (int n1 = 0; n1 < S::N1; ++n1)
+          x[i * S::N1 + n1] = csub(x[i * S::N1 + n1], cvt<FC>(ld_stream(R + (size_t)S::idxA(t, i, n1) * p.nb2)));
+    }
+    fwd_AB<S>(x, buf, tw, t, s);
+    if (s < LS) {
+      FC* out = static_cast<FC*>(p.scratch) + ((size_t)g * p.nk1 + k1) * S::N * LS + s;
+#pragma unroll
+      for (int j = 0; j < S::E2; ++j)
+#pragma unroll
+        for (int k2 = 0; k2 < S::N2; ++k2) __stcg(out + S::idxB(t, j, k2) * LS, x[j * S::N2 + k2]);
+    }
+    __syncthreads();  // buf is rewritten by the next item
+  }
+}
+
+template <typename FT, class S>
+__device__ __forceinline__ void stage_col(const FockParams& p, cpx_t<FT>* stage, int g, int k2c, int t, int s) {
+  using FC = cpx_t<FT>;
+  const int LS = p.LS;
+  const FC* col = static_cast<const FC*>(p.scratch) + ((size_t)g * p.nk1 * p.nk2 + k2c) * LS + (s < LS ? s : 0);
+  const size_t rs = (size_t)p.nk2 * LS;
+#pragma unroll
+  for (int i = 0; i < S::E1; ++i)
+#pragma unroll
+    for (int n1 = 0; n1 < S::N1; ++n1) {
+      const int n = S::idxA(t, i, n1);
+      if constexpr (sizeof(FC) == 16) cp_async16(stage + n * 16 + s, col + n * rs, s < LS);
+      else cp_async8(stage + n * 16 + s, col + n * rs, s < LS);
+    }
+  cp_async_commit();
+}
+
+template <typename ST, typename FT, class S>
+__global__ void __launch_bounds__(16 * S::TPL, 2) k_fast_col(const __grid_constant__ FockParams p) {
+  if (p.active && !*p.active) return;
+  using SC = cpx_t<ST>;
+  using FC = cpx_t<FT>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  FC* tw = reinterpret_cast<FC*>(smem_raw);
+  FC* buf = tw + S::N;
+  FC* stage = buf + 16 * S::N;
+  const int t = threadIdx.x >> 4, s = threadIdx.x & 15, LS = p.LS;
+  const int nitems = p.ngroups * p.nk2;
+  build_twiddles<FT>(tw, S::N);
+  const bool vr_scalar = (p.flags & HF_FOCK_VR_SCALAR) != 0;
+  const bool vr_real = (p.flags & HF_FOCK_VR_REAL) != 0;
+  const size_t vstride = vr_scalar ? 1 : (size_t)p.nb2;
+  const size_t rs = (size_t)p.nk2 * LS;
+  int item = blockIdx.x;
+  if (item < nitems) stage_col<FT, S>(p, stage, item % p.ngroups, item / p.ngroups, t, s);
+  __syncthreads();
+  for (; item < nitems; item += gridDim.x) {
+    const int g = item % p.ngroups, k2c = item / p.ngroups;
+    const int c = s < LS ? p.chan[g * LS + s] : -1;
+    const int vc = vr_scalar ? 0 : (c < 0 ? 0 : c);
+    // V-hat for the pattern-B frequencies of this thread, issued before the FFT
+    FT vr[S::E], vi[S::E];
+#pragma unroll
+    for (int j = 0; j < S::E2; ++j)
+#pragma unroll
+      for (int k2 = 0; k2 < S::N2; ++k2) {
+        const size_t q = (size_t)S::idxB(t, j, k2) * p.nk2 + k2c;
+        if (vr_real) {
+          vr[j * S::N2 + k2] = (FT)((double)ld_stream(static_cast<const ST*>(p.VR) + q * vstride + vc) * p.scale);
+          vi[j * S::N2 + k2] = (FT)0;
+        } else {
+          const SC z = ld_stream(static_cast<const SC*>(p.VR) + q * vstride + vc);
+          vr[j * S::N2 + k2] = (FT)((double)z.x * p.scale);
+          vi[j * S::N2 + k2] = (FT)((double)z.y * p.scale);
+        }
+      }
+    cp_async_wait_all();
+    FC x[S::E];
+#pragma unroll
+    for (int i = 0; i < S::E1; ++i)
+#pragma unroll
+      for (int n1 = 0; n1 < S::N1; ++n1) x[i * S::N1 + n1] = stage[S::idxA(t, i, n1) * 16 + s];
+    const int nx = item + gridDim.x;
+    if (nx < nitems) stage_col<FT, S>(p, stage, nx % p.ngroups, nx / p.ngroups, t, s);
+    fwd_AB<S>(x, buf, tw, t, s);
+#pragma unroll
+    for (int e = 0; e < S::E; ++e) {
+      FC v = x[e];
+      x[e] = c < 0 ? mk<FC>(0.0, 0.0) : mk<FC>(v.x * vr[e] - v.y * vi[e], v.x * vi[e] + v.y * vr[e]);
+    }
+    __syncthreads();  // buf is reused by the inverse transform
+    inv_BA<S>(x, buf, tw, t, s);
+    if (s < LS) {
+      FC* col = static_cast<FC*>(p.scratch) + ((size_t)g * p.nk1 * p.nk2 + k2c) * LS + s;
+#pragma unroll
+      for (int i = 0; i < S::E1; ++i)
+#pragma unroll
+        for (int n1 = 0; n1 < S::N1; ++n1) __stcg(col + S::idxA(t, i, n1) * rs, x[i * S::N1 + n1]);
+    }
+    __syncthreads();
+  }
+}
+
+template <typename FT, class S>
+__device__ __forceinline__ void stage_row_inv(const FockParams& p, cpx_t<FT>* stage, int g, int k1, int t, int s) {
+  using FC = cpx_t<FT>;
+  const int LS = p.LS;
+  const FC* row = static_cast<const FC*>(p.scratch) + ((size_t)g * p.nk1 + k1) * S::N * LS + (s < LS ? s : 0);
+#pragma unroll
+  for (int j = 0; j < S::E2; ++j)
+#pragma unroll
+    for (int k2 = 0; k2 < S::N2; ++k2) {
+      const int n = S::idxB(t, j, k2);
+      if constexpr (sizeof(FC) == 16) cp_async16(stage + n * 16 + s, row + n * LS, s < LS);
+      else cp_async8(stage + n * 16 + s, row + n * LS, s < LS);
+    }
+  cp_async_commit();
+}
+
+template <typename ST, typename FT, class S>
+__global__ void __launch_bounds__(16 * S::TPL, 2) k_fast_row_inv(const __grid_constant__ FockParams p) {
+  if (p.active && !*p.active) return;
+  using SC = cpx_t<ST>;
+  using FC = cpx_t<FT>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  FC* tw = reinterpret_cast<FC*>(smem_raw);
+  FC* buf = tw + S::N;
+  FC* stage = buf + 16 * S::N;
+  const int t = threadIdx.x >> 4, s = threadIdx.x & 15;
+  const int lane = threadIdx.x & 31;
+  const int LS = p.LS, nb = p.nb;
+  const int nitems = p.ngroups * p.nk1;
+  const bool exch = (p.flags & HF_FOCK_EXCHANGE) != 0;
+  const bool packing = (p.flags & HF_FOCK_PACKING) != 0;
+  const bool consts = p.sigc != nullptr;
+  const SC* h = static_cast<const SC*>(p.h);
+  SC* Sg = static_cast<SC*>(p.Sigma);
+  SC* F = static_cast<SC*>(p.F);
+  build_twiddles<FT>(tw, S::N);
+  int item = blockIdx.x;
+  if (exch && item < nitems) stage_row_inv<FT, S>(p, stage, item % p.ngroups, item / p.ngroups, t, s);
+  __syncthreads();
+  for (; item < nitems; item += gridDim.x) {
+    const int g = item % p.ngroups, k1 = item / p.ngroups;
+    const int c = s < LS ? p.chan[g * LS + s] : -1;
+    const int plane = (lane & 16) | (s < LS ? p.partner[g * LS + s] : s);
+    const int a = c >= 0 ? c / nb : 0, b = c >= 0 ? c - (c / nb) * nb : 0;
+    const size_t row0 = (size_t)k1 * S::N * p.nb2;
+    // h for this thread's k-points, issued before the transform
+    SC hv[S::E];
+#pragma unroll
+    for (int i = 0; i < S::E1; ++i)
+#pragma unroll
+      for (int m1 = 0; m1 < S::N1; ++m1)
+        hv[i * S::N1 + m1] = c >= 0 ? ld_stream(h + row0 + (size_t)S::idxA(t, i, m1) * p.nb2 + a * nb + b)
+                                    : mk<SC>(0.0, 0.0);
+    FC x[S::E];
+    if (exch) {
+      cp_async_wait_all();
+#pragma unroll
+      for (int j = 0; j < S::E2; ++j)
+#pragma unroll
+        for (int k2 = 0; k2 < S::N2; ++k2) x[j * S::N2 + k2] = stage[S::idxB(t, j, k2) * 16 + s];
+      const int nx = item + gridDim.x;
+      if (nx < nitems) stage_row_inv<FT, S>(p, stage, nx % p.ngroups, nx / p.ngroups, t, s);
+      inv_BA<S>(x, buf, tw, t, s);
+    } else {
+#pragma unroll
+      for (int e = 0; e < S::E; ++e) x[e] = mk<FC>(0.0, 0.0);
+    }
+    SC cab = mk<SC>(0.0, 0.0), cba = mk<SC>(0.0, 0.0);
+    double hd = 0.0;
+    if (consts && c >= 0) {
+      cab = cvt<SC>(p.sigc[a * nb + b]);
+      cba = cvt<SC>(p.sigc[b * nb + a]);
+      if (a == b) hd = p.hdiag[a];
+    }
+#pragma unroll
+    for (int i = 0; i < S::E1; ++i)
+#pragma unroll
+      for (int m1 = 0; m1 < S::N1; ++m1) {
+        const FC mine = x[i * S::N1 + m1];
+        const SC hab = hv[i * S::N1 + m1];
+        // every lane takes part in both shuffles (padding lanes included)
+        FC other;
+        other.x = __shfl_sync(0xffffffffu, mine.x, plane);
+        other.y = __shfl_sync(0xffffffffu, mine.y, plane);
+        SC hsh;
+        hsh.x = __shfl_sync(0xffffffffu, hab.x, plane);
+        hsh.y = __shfl_sync(0xffffffffu, hab.y, plane);
+        if (c < 0) continue;
+        const size_t base = row0 + (size_t)S::idxA(t, i, m1) * p.nb2;
+        SC sab = cvt<SC>(mine);
+        SC sba = packing ? (a == b ? sab : conj(sab)) : cvt<SC>(other);
+        sab = cadd(sab, cab);
+        sba = cadd(sba, cba);
+        const SC hba = packing ? ld_stream(h + base + b * nb + a) : hsh;
+        SC f = mk<SC>(0.5 * ((double)hab.x + (double)hba.x) + 0.5 * ((double)sab.x + (double)sba.x),
+                      0.5 * ((double)hab.y - (double)hba.y) + 0.5 * ((double)sab.y - (double)sba.y));
+        f.x += (ST)hd;
+        st_stream(Sg + base + a * nb + b, sab);
+        st_stream(F + base + a * nb + b, f);
+        if (packing && a != b) {
+          st_stream(Sg + base + b * nb + a, sba);
+          st_stream(F + base + b * nb + a, conj(f));
+        }
+      }
+    __syncthreads();
+  }
+}
+
+template <class S, typename FT>
+constexpr size_t fast_smem() {
+  return (size_t)(S::N + 32 * S::N) * sizeof(cpx_t<FT>);  // twiddles, exchange buffer, stage
+}
+
+// Persistent grid: CTAs resident on the device (2 per SM for the large shapes).
+template <typename K>
+inline int persistent_grid(K kernel, int threads, size_t smem, int items) {
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  const int g = sms * per_sm;
+  return items < g ? items : g;
+}
+
+// Launches the three passes when both mesh lengths have a fast shape; returns
+// HF_OK and sets *handled, or leaves *handled false for the generic engine.
+template <typename ST, typename FT>
+int fast_fock(FockParams& p, cudaStream_t stream, bool* handled) {
+  *handled = false;
+  if (p.LS > 16 || !fast_length(p.nk1) || !fast_length(p.nk2)) return HF_OK;
+  const bool exch = (p.flags & HF_FOCK_EXCHANGE) != 0;
+  int st = HF_OK;
+  auto row = [&](auto shape) {
+    using S = decltype(shape);
+    constexpr size_t sm = fast_smem<S, FT>();
+    if (exch) {
+      cudaFuncSetAttribute(k_fast_row_fwd<ST, FT, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      const int grid = persistent_grid(k_fast_row_fwd<ST, FT, S>, 16 * S::TPL, sm, p.ngroups * p.nk1);
+      k_fast_row_fwd<ST, FT, S><<<grid, 16 * S::TPL, sm, stream>>>(p);
+    }
+  };
+  auto col = [&](auto shape) {
+    using S = decltype(shape);
+    constexpr size_t sm = fast_smem<S, FT>();
+    cudaFuncSetAttribute(k_fast_col<ST, FT, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    const int grid = persistent_grid(k_fast_col<ST, FT, S>, 16 * S::TPL, sm, p.ngroups * p.nk2);
+    k_fast_col<ST, FT, S><<<grid, 16 * S::TPL, sm, stream>>>(p);
+  };
+  auto inv = [&](auto shape) {
+    using S = decltype(shape);
+    constexpr size_t sm = fast_smem<S, FT>();
+    cudaFuncSetAttribute(k_fast_row_inv<ST, FT, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    const int grid = persistent_grid(k_fast_row_inv<ST, FT, S>, 16 * S::TPL, sm, p.ngroups * p.nk1);
+    k_fast_row_inv<ST, FT, S><<<grid, 16 * S::TPL, sm, stream>>>(p);
+  };
+  switch (p.nk2) {
+#define HF_CASE(N, A, B, T) case N: row(LineShape<N, A, B, T>{}); break;
+    HF_FAST_SHAPES(HF_CASE)
+#undef HF_CASE
+  }
+  HF_LAUNCH_CHECK("k_fast_row_fwd");
+  if (exch) {
+    switch (p.nk1) {
+#define HF_CASE(N, A, B, T) case N: col(LineShape<N, A, B, T>{}); break;
+      HF_FAST_SHAPES(HF_CASE)
+#undef HF_CASE
+    }
+    HF_LAUNCH_CHECK("k_fast_col");
+  }
+  switch (p.nk2) {
+#define HF_CASE(N, A, B, T) case N: inv(LineShape<N, A, B, T>{}); break;
+    HF_FAST_SHAPES(HF_CASE)
+#undef HF_CASE
+  }
+  HF_LAUNCH_CHECK("k_fast_row_inv");
+  *handled = true;
+  return st;
+}
+
+}  // namespace hf

@@ -533,6 +533,7 @@ static unsigned fock_flags(const hf_cg_problem& pb, bool fp32) {
 
 struct CgRun {
   const hf_cg_problem* pb;
+  const hf_cg_config* cf;
   CgArgs a;
   void* fock_ws;
   size_t fock_ws_bytes;
@@ -552,9 +553,19 @@ static int set_smem(const void* fn, size_t bytes) {
 
 static int cg_fock(CgRun& r, cudaStream_t s, bool fp32, const int* active) {
   const hf_cg_problem& pb = *r.pb;
+  if (r.cf->fock_cb) {
+    const int st = r.cf->fock_cb(r.cf->cb_user, s, r.a.P, r.Sigma, r.H, r.a.F);
+    return st == HF_OK ? HF_OK : fail(st, "Fock-build callback failed");
+  }
   return fock_build_internal(s, HF_C128, fock_flags(pb, fp32), pb.nk1, pb.nk2, pb.nb, r.a.P, pb.h, pb.VR,
                              pb.refP, pb.HH, pb.w2d, pb.n_contact, pb.contact_g, pb.contact_Oi, pb.contact_Oj,
                              r.Sigma, r.H, r.a.F, r.fock_ws, r.fock_ws_bytes, active);
+}
+
+static int cg_project(CgRun& r, cudaStream_t s) {
+  if (!r.cf->project_cb) return HF_OK;
+  const int st = r.cf->project_cb(r.cf->cb_user, s, r.a.P);
+  return st == HF_OK ? HF_OK : fail(st, "projection callback failed");
 }
 
 static int cg_energy(CgRun& r, cudaStream_t s, double* out, const int* active) {
@@ -577,7 +588,9 @@ static int cg_iteration(CgRun& r, cudaStream_t s, const hf_cg_config& cf, bool f
   const size_t sm_den = (2 * (size_t)nb2 + nb) * 16 * kSolverWarps;
   k_cg_density<<<r.nblk, blk, sm_den, s>>>(r.a, 0);
   HF_LAUNCH_CHECK("k_cg_density");
-  int st = cg_fock(r, s, fp32, act);
+  int st = cg_project(r, s);
+  if (st) return st;
+  st = cg_fock(r, s, fp32, act);
   if (st) return st;
   st = cg_energy(r, s, &r.a.sc->E, act);
   if (st) return st;
@@ -655,6 +668,7 @@ extern "C" int hf_cg_solve(void* stream, const hf_cg_problem* pb, const hf_cg_co
 
   CgRun r;
   r.pb = pb;
+  r.cf = cf;
   CgArgs& a = r.a;
   a.nk = pb->nk1 * pb->nk2;
   a.nb = pb->nb;
@@ -679,7 +693,7 @@ extern "C" int hf_cg_solve(void* stream, const hf_cg_problem* pb, const hf_cg_co
   a.dQ = reinterpret_cast<double2*>(ws + L.off[3]);
   a.Vd = reinterpret_cast<double2*>(ws + L.off[4]);
   a.Fe = reinterpret_cast<double2*>(ws + L.off[5]);
-  r.Sigma = reinterpret_cast<double2*>(ws + L.off[6]);
+  r.Sigma = pb->sigma_buf ? static_cast<double2*>(pb->sigma_buf) : reinterpret_cast<double2*>(ws + L.off[6]);
   a.eps = reinterpret_cast<double*>(ws + L.off[7]);
   a.epsF = reinterpret_cast<double*>(ws + L.off[8]);
   a.gp0 = reinterpret_cast<double*>(ws + L.off[9]);
@@ -687,7 +701,7 @@ extern "C" int hf_cg_solve(void* stream, const hf_cg_problem* pb, const hf_cg_co
   a.dp = reinterpret_cast<double*>(ws + L.off[11]);
   a.lamd = reinterpret_cast<double*>(ws + L.off[12]);
   a.w_norm = reinterpret_cast<double*>(ws + L.off[13]);
-  r.H = reinterpret_cast<double2*>(ws + L.off[14]);
+  r.H = pb->h_buf ? static_cast<double2*>(pb->h_buf) : reinterpret_cast<double2*>(ws + L.off[14]);
   a.sc = reinterpret_cast<CgScalars*>(ws + L.off[15]);
   a.counter = reinterpret_cast<unsigned*>(ws + L.off[16]);
   a.part = reinterpret_cast<double*>(ws + L.off[17]);
@@ -748,12 +762,14 @@ extern "C" int hf_cg_solve(void* stream, const hf_cg_problem* pb, const hf_cg_co
   // ---- finalize (solver.py:613-648) ----
   k_cg_density<<<r.nblk, 32 * kSolverWarps, (2 * (size_t)nb2 + nb) * 16 * kSolverWarps, s>>>(a, 1);
   HF_LAUNCH_CHECK("k_cg_density");
+  if ((st = cg_project(r, s))) return st;
   if ((st = cg_fock(r, s, false, nullptr))) return st;
   k_cg_eig<<<r.nblk, 32 * kSolverWarps, smem_eig(nb), s>>>(a, a.F, 1);
   HF_LAUNCH_CHECK("k_cg_eig");
   if ((st = cg_mu(r, s, cf->mu_maxiter, nullptr))) return st;
   k_cg_density<<<r.nblk, 32 * kSolverWarps, (2 * (size_t)nb2 + nb) * 16 * kSolverWarps, s>>>(a, 1);
   HF_LAUNCH_CHECK("k_cg_density");
+  if ((st = cg_project(r, s))) return st;
   if ((st = cg_fock(r, s, false, nullptr))) return st;
   if ((st = cg_energy(r, s, &a.sc->E_fin, nullptr))) return st;
   k_cg_converged<<<1, 1, 0, s>>>(a);

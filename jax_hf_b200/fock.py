@@ -12,6 +12,8 @@ Differences in form, not in value:
   array with it off).
 * ``fft_precision="fp32"`` (extension) runs the exchange FFT of complex128
   inputs in FP32; everything else stays FP64.
+* ``engine="generic"`` (extension, for testing) forces the shared-memory
+  Stockham engine instead of the register FFT of the specialised mesh lengths.
 """
 
 from __future__ import annotations
@@ -47,7 +49,7 @@ def build_fock(P, *, h, VR, refP, HH, w2d, include_exchange: bool, include_hartr
                exchange_hermitian_channel_packing: bool, contact_g=None, contact_Oi=None,
                contact_Oj=None, exchange_block_specs=None, exchange_check_offdiag=None,
                exchange_offdiag_atol: float = 1e-12, exchange_offdiag_rtol: float = 0.0,
-               project_fn=None, fft_precision=None, out=None):
+               project_fn=None, fft_precision=None, engine=None, out=None):
     """Returns (Sigma, H, F) with F = herm(h + Sigma[P - refP] + H[P - refP]) (fock.py:18-97)."""
     h = _as_dev(h)
     dev = h.device
@@ -95,6 +97,8 @@ def build_fock(P, *, h, VR, refP, HH, w2d, include_exchange: bool, include_hartr
     if refP is not None and not is_marked_zero(refP):
         refPt = _as_dev(refP, dev, cdt)
         flags |= _lib.FOCK_HAS_REFP
+    if engine is not None and str(engine).lower() == "generic":
+        flags |= _lib.FOCK_GENERIC_FFT
     if fft_precision is not None and str(fft_precision).lower() in ("fp32", "float32", "single"):
         if cdt == torch.complex128:
             flags |= _lib.FOCK_FFT_FP32

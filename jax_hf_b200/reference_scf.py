@@ -1,0 +1,290 @@
+"""Reference SCF solver on the GPU (drop-in for jax_hf.reference_scf).
+
+Roothaan iteration with linear mixing, Pulay C-DIIS or ODA, optional level
+shift and trust-radius clip (reference_scf.py:31-365).  Every array operation
+runs in the CUDA library (Fock build, energy, Jacobi eigh, bisection mu,
+occupations, residuals/commutators, DIIS Gram matrix, extrapolation); the
+loop's scalar decisions are taken on the host from a few float64 reductions per
+iteration, as the reference does in its traced loop.  The (N+1)^2 bordered DIIS
+system is solved on the host with LAPACK (numpy), like jnp.linalg.solve on CPU.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Any, Callable
+
+import numpy as np
+import torch
+
+from . import _lib
+from .fock import build_fock, hf_energy
+from .linalg import eigh, density_from_Qp
+from .utils import validate_electron_count
+
+
+@dataclass(frozen=True)
+class SCFConfig:
+    """reference_scf.py:31-63 (same fields, defaults and validation)."""
+    max_iter: int = 200
+    density_tol: float = 1e-7
+    comm_tol: float = 1e-6
+    mixing: float = 0.5
+    level_shift: float = 0.0
+    acceleration: str = "linear"
+    diis_size: int = 6
+    diis_start: int = 2
+    diis_damping: float = 1.0
+    trust_radius: float = 0.0
+    project_fn: Callable[[Any], Any] | None = None
+
+    def __post_init__(self) -> None:
+        if self.max_iter <= 0:
+            raise ValueError("max_iter must be positive")
+        if self.acceleration not in ("linear", "diis", "oda"):
+            raise ValueError("SCFConfig.acceleration must be 'linear', 'diis', or 'oda'; "
+                             f"got {self.acceleration!r}")
+        if self.diis_size <= 0:
+            raise ValueError("diis_size must be positive")
+
+
+@dataclass(frozen=True)
+class SCFResult:
+    density_matrix: Any
+    fock_matrix: Any
+    energy: Any
+    chemical_potential: Any
+    iterations: int
+    converged: bool
+    message: str
+    history: dict[str, Any] = field(default_factory=dict)
+
+
+class _Ops:
+    """Thin wrappers of the C-ABI operations on complex128 / float64 tensors."""
+
+    def __init__(self, device, nk1, nk2, nb):
+        self.dev = device
+        self.nk = nk1 * nk2
+        self.nk1, self.nk2, self.nb = nk1, nk2, nb
+        L = _lib.lib()
+        self.L = L
+        n = C.c_size_t(0)
+        _lib.check(L.hf_ops_workspace_size(C.byref(n)))
+        self.ws = torch.empty(n.value, dtype=torch.uint8, device=device)
+        self.red = torch.empty(64, dtype=torch.float64, device=device)
+        self.s = _lib.stream_ptr(device)
+
+    def herm(self, X, out=None, a=1.0, Y=None, b=0.0):
+        out = torch.empty_like(X) if out is None else out
+        _lib.check(self.L.hf_axpby(self.s, self.nk, self.nb, a, X.data_ptr(), b, _lib.ptr(Y), 1, out.data_ptr()))
+        return out
+
+    def fermi(self, eps, mu, T, mode, shift=0.0, out=None):
+        out = torch.empty_like(eps) if out is None else out
+        _lib.check(self.L.hf_fermi(self.s, eps.numel(), eps.data_ptr(), mu.data_ptr(), float(T), mode, float(shift),
+                                   out.data_ptr()))
+        return out
+
+    def find_mu(self, eps, w, n_electrons, T, method=0, mu0=None, out=None):
+        out = torch.empty((), dtype=torch.float64, device=self.dev) if out is None else out
+        _lib.check(self.L.hf_find_mu(self.s, _lib.HF_C128, method, self.nk, 1, self.nb, eps.data_ptr(), w.data_ptr(),
+                                     float(n_electrons), float(T), 0, _lib.ptr(mu0), out.data_ptr()))
+        return out
+
+
+def solve_scf(kernel, P0, n_electrons: float, *, config: SCFConfig | None = None,
+              fock_build_fn: Callable | None = None) -> SCFResult:
+    """Reference SCF solver (reference_scf.py:124-219)."""
+    if config is None:
+        config = SCFConfig()
+    cfg = config
+    dev = kernel.device
+    nk1, nk2, nb = kernel.shape
+    cd = torch.complex128
+    h = kernel.h.to(cd)
+    w2d = kernel.w2d.to(torch.float64).contiguous()
+    ws = max(float(kernel.weight_sum), 1e-30)
+    T = float(kernel.T)
+    ops = _Ops(dev, nk1, nk2, nb)
+    project = cfg.project_fn
+    validate_electron_count(w2d, nb, n_electrons, context="n_electrons")
+    a = kernel.as_args()
+    VR = a["VR"] if kernel.dtype == cd else (a["VR"].to(cd) if a["VR"].is_complex() else a["VR"].to(torch.float64))
+    fock_kw = dict(h=h, VR=VR, refP=kernel.refP if kernel.dtype == cd else kernel.refP.to(cd), HH=kernel.HH.double(),
+                   w2d=w2d, include_exchange=kernel.include_exchange, include_hartree=kernel.include_hartree,
+                   exchange_hermitian_channel_packing=kernel.exchange_hermitian_channel_packing,
+                   contact_g=kernel.contact_g.double(), contact_Oi=kernel.contact_Oi.to(cd),
+                   contact_Oj=kernel.contact_Oj.to(cd))
+    if kernel.dtype == cd:
+        fock_kw["refP"] = kernel.refP
+        fock_kw["contact_g"] = kernel.contact_g
+        fock_kw["contact_Oi"] = kernel.contact_Oi
+        fock_kw["contact_Oj"] = kernel.contact_Oj
+    fn = fock_build_fn or build_fock
+
+    def proj_herm(X):
+        if project is None:
+            return ops.herm(X)
+        return ops.herm(torch.as_tensor(project(X)).to(cd).contiguous())
+
+    def fock(P):
+        return fn(P, project_fn=project, **fock_kw)
+
+    def density_from_fock(F):
+        """reference_scf.py:87-96: eigh, bisection mu, level shift, occupations."""
+        ev, orb = eigh(F)
+        mu_raw = ops.find_mu(ev, w2d, n_electrons, T, method=0)
+        if cfg.level_shift != 0.0:
+            shifted = ops.fermi(ev, mu_raw, T, 2, cfg.level_shift)
+            mu = ops.find_mu(shifted, w2d, n_electrons, T, method=0)
+        else:
+            shifted, mu = ev, mu_raw
+        occ = ops.fermi(shifted, mu, T, 0)
+        return density_from_Qp(orb, occ), mu
+
+    def build_and_occupy(dens):
+        dh = proj_herm(dens)
+        Sg, Hh, F = fock(dh)
+        E = hf_energy(dh, h=h, Sigma=Sg, H=Hh, weights_b=w2d)
+        Pn, mu = density_from_fock(F)
+        if project is not None:
+            Pn = proj_herm(Pn)
+        return Pn, F, E, mu
+
+    use_diis = cfg.acceleration == "diis"
+    n_hist = cfg.diis_size if use_diis else 0
+    if use_diis:
+        F_hist = torch.zeros((n_hist, nk1, nk2, nb, nb), dtype=cd, device=dev)
+        R_hist = torch.zeros_like(F_hist)
+        stride = nk1 * nk2 * nb * nb
+    comm_buf = torch.empty((nk1, nk2, nb, nb), dtype=cd, device=dev)
+    delta = torch.empty_like(comm_buf)
+    sums = torch.empty(3, dtype=torch.float64, device=dev)
+    gram = torch.empty(64, dtype=torch.float64, device=dev)
+    coeff_dev = torch.empty(max(n_hist, 1), dtype=torch.float64, device=dev)
+    hE, hD, hC = [], [], []
+    density = torch.as_tensor(P0).to(dev, cd).contiguous() if not (
+        isinstance(P0, torch.Tensor) and P0.dtype == cd) else P0.to(dev).contiguous()
+    k, converged = 0, False
+    while k < cfg.max_iter and not converged:
+        P_new, F, E, mu = build_and_occupy(density)
+        R_out = R_hist[k % n_hist] if use_diis else comm_buf
+        _lib.check(ops.L.hf_scf_residuals(ops.s, ops.nk, nb, F.data_ptr(), density.data_ptr(), P_new.data_ptr(),
+                                          w2d.data_ptr(), R_out.data_ptr(), delta.data_ptr(), sums.data_ptr(),
+                                          ops.ws.data_ptr()))
+        s_host = sums.cpu().numpy()
+        E_host = float(E)
+        d_res = float(np.sqrt(s_host[0] / ws))
+        c_res = float(np.sqrt(s_host[1] / ws))
+        converged = d_res <= cfg.density_tol and c_res <= cfg.comm_tol
+        if use_diis:
+            idx = k % n_hist
+            F_hist[idx].copy_(F)
+            count = min(k + 1, n_hist)
+            active = (np.arange(n_hist) < count).astype(np.float64)
+            B = _gram_matrix(ops, R_hist, n_hist, stride, w2d, gram)
+            B = B / max(np.max(np.abs(B)), 1e-30)
+            A = np.zeros((n_hist + 1, n_hist + 1))
+            A[:n_hist, :n_hist] = B + np.diag(1.0 - active)
+            A[:n_hist, n_hist] = -active
+            A[n_hist, :n_hist] = -active
+            rhs = np.zeros(n_hist + 1)
+            rhs[n_hist] = -1.0
+            try:
+                sol = np.linalg.solve(A, rhs)
+            except np.linalg.LinAlgError:
+                sol = np.full(n_hist + 1, np.nan)
+            coeffs = sol[:n_hist]
+            ok = bool(np.all(np.isfinite(sol)))
+            engaged = count >= max(2, cfg.diis_start) and ok
+            if engaged:
+                coeff_dev.copy_(torch.from_numpy(coeffs))
+                Fx = torch.empty_like(F)
+                _lib.check(ops.L.hf_lincomb(ops.s, n_hist, stride, stride, F_hist.data_ptr(), coeff_dev.data_ptr(),
+                                            Fx.data_ptr()))
+                damp = float(np.clip(cfg.diis_damping, 0.0, 1.0))
+                if damp != 1.0:
+                    Fd = torch.empty_like(F)
+                    _lib.check(ops.L.hf_axpby(ops.s, ops.nk, nb, damp, Fx.data_ptr(), 1.0 - damp, F.data_ptr(), 0,
+                                              Fd.data_ptr()))
+                    Fx = Fd
+                Pd, _ = density_from_fock(ops.herm(Fx))
+                updated = proj_herm(Pd) if project is not None else Pd
+            else:
+                updated = _linear(ops, density, delta, cfg.mixing, project, proj_herm)
+        elif cfg.acceleration == "oda":
+            Sn, Hn, _ = fock(P_new)
+            E_new = float(hf_energy(P_new, h=h, Sigma=Sn, H=Hn, weights_b=w2d))
+            c1 = float(s_host[2])
+            c2 = (E_new - E_host) - c1
+            if c2 > 1e-12:
+                lam = float(np.clip(-c1 / (2.0 * c2), 0.0, 1.0))
+            else:
+                lam = 1.0 if c1 < 0.0 else 0.0
+            updated = proj_herm_axpy(ops, density, delta, lam, project, proj_herm)
+        else:
+            updated = _linear(ops, density, delta, cfg.mixing, project, proj_herm)
+        if cfg.trust_radius > 0.0:                              # reference_scf.py:333-339
+            step = torch.empty_like(density)
+            _lib.check(ops.L.hf_axpby(ops.s, ops.nk, nb, 1.0, updated.data_ptr(), -1.0, density.data_ptr(), 0,
+                                      step.data_ptr()))
+            _lib.check(ops.L.hf_jdot(ops.s, ops.nk, nb, step.data_ptr(), step.data_ptr(), w2d.data_ptr(), None, None,
+                                     None, ops.red.data_ptr(), ops.ws.data_ptr()))
+            sn = float(np.sqrt(float(ops.red[0]) / ws))
+            if sn > cfg.trust_radius:
+                scale = cfg.trust_radius / max(sn, 1e-30)
+                updated = proj_herm_axpy(ops, density, step, scale, project, proj_herm)
+        density = P_new if converged else updated
+        hE.append(E_host)
+        hD.append(d_res)
+        hC.append(c_res)
+        k += 1
+    _, F_fin, E_fin, mu_fin = build_and_occupy(density)
+    n_iter = k
+    if converged:
+        message = f"converged in {n_iter} iterations"
+    else:
+        dr = hD[-1] if n_iter > 0 else float("nan")
+        cr = hC[-1] if n_iter > 0 else float("nan")
+        message = f"stopped after {n_iter} iterations (density_res={dr:.3e}, comm_res={cr:.3e})"
+    out_c = kernel.dtype
+    return SCFResult(density_matrix=density.to(out_c), fock_matrix=F_fin.to(out_c), energy=E_fin,
+                     chemical_potential=mu_fin, iterations=n_iter, converged=bool(converged), message=message,
+                     history={"E": np.asarray(hE), "density_residual": np.asarray(hD),
+                              "commutator_residual": np.asarray(hC)})
+
+
+def _linear(ops, density, delta, mixing, project, proj_herm):
+    """herm(project(density + mixing * delta)) (reference_scf.py:275-276)."""
+    return proj_herm_axpy(ops, density, delta, mixing, project, proj_herm)
+
+
+def proj_herm_axpy(ops, X, Y, b, project, proj_herm):
+    if project is None:
+        return ops.herm(X, a=1.0, Y=Y, b=b)
+    tmp = torch.empty_like(X)
+    _lib.check(ops.L.hf_axpby(ops.s, ops.nk, ops.nb, 1.0, X.data_ptr(), b, Y.data_ptr(), 0, tmp.data_ptr()))
+    return proj_herm(tmp)
+
+
+def _gram_matrix(ops, R_hist, n, stride, w2d, gram):
+    """B_ij = sum_k w Re tr(R_i^H R_j) over all n history slots (reference_scf.py:110-111)."""
+    B = np.zeros((n, n))
+    if n <= 6:
+        _lib.check(ops.L.hf_gram(ops.s, n, stride, ops.nk, ops.nb, R_hist.data_ptr(), w2d.data_ptr(),
+                                 gram.data_ptr(), ops.ws.data_ptr()))
+        g = gram[: n * (n + 1) // 2].cpu().numpy()
+        q = 0
+        for i in range(n):
+            for j in range(i, n):
+                B[i, j] = B[j, i] = g[q]
+                q += 1
+        return B
+    for i in range(n):
+        for j in range(i, n):
+            _lib.check(ops.L.hf_jdot(ops.s, ops.nk, ops.nb, R_hist[i].data_ptr(), R_hist[j].data_ptr(),
+                                     w2d.data_ptr(), None, None, None, gram.data_ptr(), ops.ws.data_ptr()))
+            B[i, j] = B[j, i] = float(gram[0])
+    return B

@@ -70,7 +70,12 @@ class _CgProblem(C.Structure):
                 ("T", C.c_double), ("n_electrons", C.c_double), ("weight_sum", C.c_double),
                 ("h", C.c_void_p), ("VR", C.c_void_p), ("refP", C.c_void_p), ("HH", C.c_void_p),
                 ("w2d", C.c_void_p), ("n_contact", C.c_int), ("contact_g", C.c_void_p),
-                ("contact_Oi", C.c_void_p), ("contact_Oj", C.c_void_p)]
+                ("contact_Oi", C.c_void_p), ("contact_Oj", C.c_void_p), ("sigma_buf", C.c_void_p),
+                ("h_buf", C.c_void_p)]
+
+
+FOCK_CB = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p)
+PROJECT_CB = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_void_p)
 
 
 class _CgConfig(C.Structure):
@@ -78,7 +83,7 @@ class _CgConfig(C.Structure):
                 ("denom_scale", C.c_double), ("max_step", C.c_double), ("cg_restart", C.c_int),
                 ("bt_shrink", C.c_double), ("bt_max", C.c_int), ("mu_maxiter", C.c_int),
                 ("plateau_window", C.c_int), ("fp32_exchange", C.c_int), ("fp32_switch_rel", C.c_double),
-                ("chunk", C.c_int)]
+                ("chunk", C.c_int), ("fock_cb", FOCK_CB), ("project_cb", PROJECT_CB), ("cb_user", C.c_void_p)]
 
 
 def _bind():
@@ -135,13 +140,18 @@ class KernelC128:
         return _CgProblem(nk1, nk2, nb, self.flags(), float(k.T), float(n_electrons), float(k.weight_sum),
                           self.h.data_ptr(), self.VR.data_ptr(), _lib.ptr(self.refP), self.HH.data_ptr(),
                           self.w2d.data_ptr(), int(self.cg.shape[0]) if self.has_contact else 0,
-                          self.cg.data_ptr(), self.cOi.data_ptr(), self.cOj.data_ptr())
+                          self.cg.data_ptr(), self.cOi.data_ptr(), self.cOj.data_ptr(), None, None)
+
+    def fock_kwargs(self):
+        k = self.kernel
+        return dict(h=self.h, VR=self.VR, refP=k.refP if self.refP is None else self.refP, HH=self.HH, w2d=self.w2d,
+                    include_exchange=k.include_exchange, include_hartree=k.include_hartree,
+                    exchange_hermitian_channel_packing=k.exchange_hermitian_channel_packing,
+                    contact_g=k.contact_g if not self.has_contact else self.cg,
+                    contact_Oi=self.cOi, contact_Oj=self.cOj)
 
 
 def _solve_cg(kernel, P0, n_electrons, cfg: SolverConfig, fock_build_fn=None):
-    if cfg.project_fn is not None or cfg.block_sizes is not None or fock_build_fn is not None:
-        from .solver_host import solve_cg_host
-        return solve_cg_host(kernel, P0, n_electrons, cfg, fock_build_fn)
     L = _bind()
     dev = kernel.device
     nk1, nk2, nb = kernel.shape
@@ -150,7 +160,7 @@ def _solve_cg(kernel, P0, n_electrons, cfg: SolverConfig, fock_build_fn=None):
     conf = _CgConfig(int(cfg.max_iter), float(cfg.tol_E), float(cfg.tol_grad), float(cfg.denom_scale),
                      float(cfg.max_step), int(cfg.cg_restart), float(cfg.bt_shrink), int(cfg.bt_max),
                      int(cfg.mu_maxiter), int(cfg.plateau_window), int(bool(cfg.fp32_exchange)),
-                     float(cfg.fp32_switch_rel), int(cfg.chunk))
+                     float(cfg.fp32_switch_rel), int(cfg.chunk), FOCK_CB(), PROJECT_CB(), None)
     need = C.c_size_t(0)
     _lib.check(L.hf_cg_workspace_size(C.byref(prob), C.byref(conf), C.byref(need)))
     ws = torch.empty(need.value, dtype=torch.uint8, device=dev)
@@ -163,9 +173,52 @@ def _solve_cg(kernel, P0, n_electrons, cfg: SolverConfig, fock_build_fn=None):
     hE = torch.zeros(max(cfg.max_iter, 1), dtype=torch.float64, device=dev)
     hG = torch.zeros(max(cfg.max_iter, 1), dtype=torch.float64, device=dev)
     sc = torch.zeros(8, dtype=torch.float64, device=dev)
-    _lib.check(L.hf_cg_solve(_lib.stream_ptr(dev), C.byref(prob), C.byref(conf), P0t.data_ptr(), Q.data_ptr(),
+    errors = []
+    if cfg.project_fn is not None or cfg.block_sizes is not None or fock_build_fn is not None:
+        # Python hooks: the loop stays on the device, the callbacks enqueue their work on the same stream
+        Sg_t = torch.empty_like(Q)
+        H_t = torch.zeros((nb, nb), dtype=torch.complex128, device=dev)
+        prob.sigma_buf, prob.h_buf = Sg_t.data_ptr(), H_t.data_ptr()
+        fn = fock_build_fn
+        if fn is None:
+            from .fock import build_fock as fn
+        specs = None if cfg.block_sizes is None else (("sizes", tuple(int(s) for s in cfg.block_sizes)),)
+        fkw = kc.fock_kwargs()
+        calls = [0]
+
+        def fock_cb(user, stream, Pp, Sp, Hp, Fp):
+            try:
+                first = calls[0] == 0
+                calls[0] += 1
+                Sg, Hh, Fn = fn(P, exchange_block_specs=specs, project_fn=cfg.project_fn if first else None, **fkw)
+                Sg_t.copy_(Sg)
+                Hh = torch.as_tensor(Hh).to(dev, torch.complex128)
+                H_t.copy_(Hh.reshape(-1, nb, nb)[0] if Hh.numel() >= nb * nb else Hh.expand(nb, nb))
+                F.copy_(Fn)
+                return 0
+            except Exception as exc:  # re-raised after the C call returns
+                errors.append(exc)
+                return _lib.HF_ERR_ABORTED
+
+        def project_cb(user, stream, Pp):
+            try:
+                X = torch.as_tensor(cfg.project_fn(P)).to(dev, torch.complex128)
+                P.copy_(0.5 * (X + X.transpose(-1, -2).conj()))
+                return 0
+            except Exception as exc:
+                errors.append(exc)
+                return _lib.HF_ERR_ABORTED
+
+        conf.fock_cb = FOCK_CB(fock_cb)
+        if cfg.project_fn is not None:
+            conf.project_cb = PROJECT_CB(project_cb)
+        _keep = (conf.fock_cb, conf.project_cb)
+    st = L.hf_cg_solve(_lib.stream_ptr(dev), C.byref(prob), C.byref(conf), P0t.data_ptr(), Q.data_ptr(),
                              p.data_ptr(), P.data_ptr(), F.data_ptr(), hE.data_ptr(), hG.data_ptr(), sc.data_ptr(),
-                             ws.data_ptr(), ws.numel()))
+                             ws.data_ptr(), ws.numel())
+    if errors:
+        raise errors[0]
+    _lib.check(st)
     out_c = kernel.dtype
     out_r = kernel.real_dtype
     s = sc.cpu().numpy()

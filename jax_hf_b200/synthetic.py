@@ -66,7 +66,7 @@ def hamiltonian_from_coeffs(coeffs, nk: int):
     H = np.zeros((nk, nk, nb, nb), np.complex128)
     for R, hR in coeffs.items():
         H += np.exp(1j * (kx * R[0] + ky * R[1]))[..., None, None] * hR[None, None]
-    return 0.5 * (H + np.conj(np.swapaxes(H, -1, -2)))
+    return np.ascontiguousarray(0.5 * (H + np.conj(np.swapaxes(H, -1, -2))))
 
 
 def _qabs(nk: int):
@@ -107,7 +107,7 @@ def haar_density(nk: int, nb: int, seed: int):
     U = haar_unitaries((nk, nk), nb, rng)
     f = rng.uniform(0.0, 1.0, size=(nk, nk, nb))
     P = np.einsum("...in,...n,...jn->...ij", U, f, np.conj(U))
-    return 0.5 * (P + np.conj(np.swapaxes(P, -1, -2)))
+    return np.ascontiguousarray(0.5 * (P + np.conj(np.swapaxes(P, -1, -2))))
 
 
 @dataclass
