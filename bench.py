@@ -242,12 +242,11 @@ def _finish(args, ws, rank, value, dev_ms, avg_us, n_builds, t_wall, clocks, var
     ab = alg_bytes(NK, NK, NB)
     achieved = ab / (avg_us * 1e-6) / 1e9
     traffic = None
-    tf = ROOT / "profiles" / "fock_build_192x192_nb8_c128_traffic.json"
+    tf = ROOT / "profiles" / "fock_build_192x192_nb8_c128_fast_passes.md"
     if tf.exists():
-        try:
-            traffic = json.loads(tf.read_text()).get("dram_bytes_per_build")
-        except Exception:
-            traffic = None
+        for ln in tf.read_text().splitlines():
+            if ln.strip().startswith("traffic_bytes_per_build:"):
+                traffic = int(ln.split(":")[1])
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(dev_ms / args.steps, 4), "higher_is_better": True,
