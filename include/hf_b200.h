@@ -259,6 +259,33 @@ int hf_cg_solve(void* stream, const hf_cg_problem* problem, const hf_cg_config* 
                 void* Q, void* p, void* density, void* fock, double* hist_E, double* hist_grad,
                 double* scalars_out, void* workspace, size_t workspace_bytes);
 
+/* Batched density scan: many independent CG solves, no host callbacks.  The
+ * solves are ordered longest first (nk * nb^2 * (nb + 8)) and run n_lanes at a
+ * time, each lane on its own stream (ordered after `stream`, which waits for all
+ * of them at the end) with its iterations replayed from CUDA graphs; the host
+ * thread polls events and feeds a free lane the next solve.  Each item has the
+ * outputs of hf_cg_solve.  workspace = n_lanes * bytes_per_lane bytes
+ * (bytes_per_lane from hf_cg_batch_workspace_size).  solve_ms (host, n_items,
+ * may be NULL) receives each solve's device time from its start to its final
+ * scalars.  Extension of the reference API (the reference runs solves one by
+ * one from Python, e.g. benchmarks/ and continuation.py loops). */
+typedef struct hf_cg_batch_item {
+  hf_cg_problem problem;
+  const void* P0;
+  void* Q;
+  void* p;
+  void* density;
+  void* fock;
+  double* hist_E;      /* may be NULL */
+  double* hist_grad;   /* may be NULL */
+  double* scalars_out; /* device, 8 float64 as for hf_cg_solve */
+} hf_cg_batch_item;
+
+int hf_cg_batch_workspace_size(const hf_cg_batch_item* items, int n_items, const hf_cg_config* config,
+                               size_t* bytes_per_lane);
+int hf_cg_solve_batch(void* stream, const hf_cg_batch_item* items, int n_items, const hf_cg_config* config,
+                      int n_lanes, void* workspace, size_t bytes_per_lane, double* solve_ms);
+
 #ifdef __cplusplus
 }
 #endif

@@ -73,6 +73,8 @@ _SIGS = {
     "hf_real_diag": ([vp, sz, i32, vp, vp], i32),
     "hf_cg_workspace_size": ([vp, vp, psz], i32),
     "hf_cg_solve": ([vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, sz], i32),
+    "hf_cg_batch_workspace_size": ([vp, i32, vp, psz], i32),
+    "hf_cg_solve_batch": ([vp, vp, i32, vp, i32, vp, sz, vp], i32),
 }
 
 

@@ -1,4 +1,6 @@
 // Error reporting and version of the hf_b200 C ABI.
+#include <mutex>
+#include <set>
 #include <string>
 
 #include "common.cuh"
@@ -17,6 +19,26 @@ int fail(int status, const std::string& msg) {
 int cuda_check(cudaError_t e, const char* what) {
   g_last_error = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
   return HF_ERR_CUDA;
+}
+
+// Lifts a kernel's dynamic shared-memory cap to the device's opt-in maximum, once
+// per (kernel, device).  The cap only bounds launches (occupancy follows each
+// launch's own size); a per-call cap could drop below the size of a launch that
+// another stream (a batch lane, a captured graph) still has to make.
+int allow_max_dynamic_smem(const void* fn) {
+  static std::mutex mu;
+  static std::set<std::pair<const void*, int>> done;
+  int dev = 0;
+  HF_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  if (done.count({fn, dev})) return HF_OK;
+  int optin = 0;
+  HF_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  cudaFuncAttributes fa;
+  HF_CUDA(cudaFuncGetAttributes(&fa, fn));
+  HF_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes));
+  done.insert({fn, dev});
+  return HF_OK;
 }
 
 }  // namespace hf

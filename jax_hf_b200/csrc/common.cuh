@@ -14,6 +14,13 @@ namespace hf {
 void set_error(const std::string& msg);
 int fail(int status, const std::string& msg);
 int cuda_check(cudaError_t e, const char* what);
+int allow_max_dynamic_smem(const void* fn);
+
+#define HF_SMEM_CAP(...)                                              \
+  do {                                                                \
+    const int _st = ::hf::allow_max_dynamic_smem((const void*)(__VA_ARGS__));  \
+    if (_st) return _st;                                              \
+  } while (0)
 
 #define HF_CUDA(call)                                            \
   do {                                                           \

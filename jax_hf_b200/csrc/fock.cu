@@ -433,9 +433,9 @@ static int launch_fock(FockParams& p, cudaStream_t stream, bool need_consts) {
   const bool exch = (p.flags & HF_FOCK_EXCHANGE) != 0;
   const size_t sm_row = fock_smem_bytes<FT>(p.nk2, p.LS);
   const size_t sm_col = fock_smem_bytes<FT>(p.nk1, p.LS);
-  HF_CUDA(cudaFuncSetAttribute(k_fock_row_fwd<ST, FT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_row));
-  HF_CUDA(cudaFuncSetAttribute(k_fock_col<ST, FT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_col));
-  HF_CUDA(cudaFuncSetAttribute(k_fock_row_inv<ST, FT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_row));
+  HF_SMEM_CAP(k_fock_row_fwd<ST, FT>);
+  HF_SMEM_CAP(k_fock_col<ST, FT>);
+  HF_SMEM_CAP(k_fock_row_inv<ST, FT>);
   dim3 grow(p.nk1, p.ngroups), gcol(p.nk2, p.ngroups);
   if (need_consts) {
     k_fock_rho_part<ST><<<grow, kThreads, 0, stream>>>(p);

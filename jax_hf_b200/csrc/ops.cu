@@ -410,7 +410,7 @@ extern "C" int hf_scf_residuals(void* stream, int nk, int nb, const void* F, con
   if (!F || !P || !Pn || !w || !sums3 || !ws || nb > 32) return fail(HF_ERR_INVALID, "hf_scf_residuals: bad argument");
   const int g = perk_grid(nk);
   const size_t sm = (size_t)3 * nb * nb * sizeof(double2) * 4;
-  HF_CUDA(cudaFuncSetAttribute(k_scf_residuals, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  HF_SMEM_CAP(k_scf_residuals);
   k_scf_residuals<<<g, 128, sm, HF_S>>>(nk, nb, (const double2*)F, (const double2*)P, (const double2*)Pn, w,
                                         (double2*)comm, (double2*)delta, (double*)ws);
   return finish(HF_S, (double*)ws, g, 3, sums3);
@@ -487,7 +487,7 @@ extern "C" int hf_newton_dP(void* stream, int nk, int nb, const void* Q, const v
                             const double* p, void* dP) {
   if (!Q || !X || !dp || !p || !dP || nb > 32) return fail(HF_ERR_INVALID, "hf_newton_dP: bad argument");
   const size_t sm = (size_t)3 * nb * nb * sizeof(double2) * 4;
-  HF_CUDA(cudaFuncSetAttribute(k_newton_dP, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  HF_SMEM_CAP(k_newton_dP);
   k_newton_dP<<<perk_grid(nk), 128, sm, HF_S>>>(nk, nb, (const double2*)Q, (const double2*)X, dp, p, (double2*)dP);
   HF_LAUNCH_CHECK("k_newton_dP");
   return HF_OK;
@@ -501,7 +501,7 @@ extern "C" int hf_newton_hvp(void* stream, int nk, int nb, const void* Q, const 
     return fail(HF_ERR_INVALID, "hf_newton_hvp: bad argument");
   const int g = perk_grid(nk);
   const size_t sm = (size_t)5 * nb * nb * sizeof(double2) * 4;
-  HF_CUDA(cudaFuncSetAttribute(k_newton_hvp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  HF_SMEM_CAP(k_newton_hvp);
   k_newton_hvp<<<g, 128, sm, HF_S>>>(nk, nb, (const double2*)Q, (const double2*)Ft, (const double2*)X, dp, p,
                                      (const double2*)Fr, (const double2*)h, T, clipv, pen, (const double2*)dPpen,
                                      (double2*)HX, Hp, w2d, (double*)ws);
@@ -511,7 +511,7 @@ extern "C" int hf_newton_hvp(void* stream, int nk, int nb, const void* Q, const 
 extern "C" int hf_matmul(void* stream, int nk, int nb, const void* A, const void* B, void* C) {
   if (!A || !B || !C || nb > 32) return fail(HF_ERR_INVALID, "hf_matmul: bad argument");
   const size_t sm = (size_t)2 * nb * nb * sizeof(double2) * 4;
-  HF_CUDA(cudaFuncSetAttribute(k_matmul, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  HF_SMEM_CAP(k_matmul);
   k_matmul<<<perk_grid(nk), 128, sm, HF_S>>>(nk, nb, (const double2*)A, (const double2*)B, (double2*)C);
   HF_LAUNCH_CHECK("k_matmul");
   return HF_OK;

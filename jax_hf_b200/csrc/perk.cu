@@ -232,7 +232,7 @@ static Launch warp_launch(int batch, size_t per_warp_elems) {
   return L;
 }
 
-#define HF_SET_SMEM(kern, L) HF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(L).smem))
+#define HF_SET_SMEM(kern, L) HF_SMEM_CAP(kern)
 
 }  // namespace hf
 

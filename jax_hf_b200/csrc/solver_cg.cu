@@ -12,7 +12,9 @@
 // ticket), which also performs the scalar update of the reference loop body.
 // Every kernel of an iteration returns at once when the device flag `active`
 // is clear, so whole chunks can be queued without host round trips.
+#include <algorithm>
 #include <cmath>
+#include <thread>
 #include <vector>
 
 #include "common.cuh"
@@ -52,6 +54,12 @@ struct CgArgs {
 };
 
 __device__ __forceinline__ bool cg_active(const CgArgs& a) { return a.sc->active != 0; }
+
+}  // namespace hf
+
+#include "cg_rows.cuh"  // lane-per-row kernels (use CgArgs / cg_active above)
+
+namespace hf {
 
 // ------------------------------------------------------------------ init ---
 __global__ void k_cg_init(CgArgs a, const double2* __restrict__ P0, const double* __restrict__ w2d,
@@ -229,7 +237,7 @@ __global__ void k_cg_grad1(CgArgs a) {
     __syncwarp();
   }
   if (publish_partials<4>(acc, a.part, a.counter, red)) {
-    gather_partials<4>(a.part, a.counter, tot);
+    gather_partials<4>(a.part, a.counter, tot, red);
     if (threadIdx.x == 0) {
       CgScalars* s = a.sc;
       s->grad_norm = sqrt(fmax(0.0, tot[0]));
@@ -278,7 +286,7 @@ __global__ void k_cg_grad2(CgArgs a) {
     }
   }
   if (publish_partials<4>(acc, a.part, a.counter, red)) {
-    gather_partials<4>(a.part, a.counter, tot);
+    gather_partials<4>(a.part, a.counter, tot, red);
     if (threadIdx.x == 0) {
       CgScalars* s = a.sc;
       const double num = tot[0] - tot[1] + tot[2] - tot[3];
@@ -358,7 +366,50 @@ __global__ void k_cg_dir(CgArgs a) {
     __syncwarp();
   }
   if (publish_partials<3>(acc, a.part, a.counter, red)) {
-    gather_partials<3>(a.part, a.counter, tot);
+    gather_partials<3>(a.part, a.counter, tot, red);
+    if (threadIdx.x == 0) {
+      CgScalars* s = a.sc;
+      const double dn = sqrt(fmax(0.0, tot[0]));
+      s->tau0 = fmin(1.0, a.max_step / fmax(dn, 1e-30));
+      s->Omega0 = tot[1] + fmax(a.T_r, 1e-14) * tot[2];
+      s->accepted = 0;
+      s->tau_final = s->tau0;
+    }
+  }
+}
+
+// ---- direction d = H + beta d_prev (elementwise), tau0 and Omega0: the retraction
+// of the lane-per-row path needs no eigendecomposition of d.
+__global__ void k_cg_dir_lu(CgArgs a) {
+  if (!cg_active(a)) return;
+  __shared__ double red[64];
+  __shared__ double tot[kMaxSums];
+  const int par = a.sc->k & 1;
+  const double2* G = par ? a.G1 : a.G0;
+  const double* gp = par ? a.gp1 : a.gp0;
+  const double lam = a.sc->lam, beta = a.sc->beta;
+  const unsigned nb = a.nb, nb2 = nb * nb;
+  const unsigned nq = (unsigned)a.nk * nb2, nv = (unsigned)a.nk * nb;
+  KSum acc[3];
+  for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < nq; e += gridDim.x * blockDim.x) {
+    const unsigned k = e / nb2, rr = e - k * nb2, i = rr / nb, j = rr - i * nb;
+    const double2 hq = precond(G[e], a.epsF[k * nb + i], a.epsF[k * nb + j], lam);
+    const double2 dprev = a.dQ[e];
+    const double2 d = make_double2(hq.x + beta * dprev.x, hq.y + beta * dprev.y);
+    a.dQ[e] = d;
+    acc[0].add(a.w_norm[k] * (d.x * d.x + d.y * d.y));
+  }
+  for (unsigned v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
+    const unsigned k = v / nb;
+    const double wk = a.w_norm[k];
+    const double ps = clip(a.p[v], 1e-8, 1.0 - 1e-8);
+    const double hp = gp[v] * (ps * (1.0 - ps) / a.T_r);
+    a.dp[v] = hp + beta * a.dp[v];
+    acc[1].add(wk * ps * a.epsF[v]);
+    acc[2].add(wk * ent_term(ps));
+  }
+  if (publish_partials<3>(acc, a.part, a.counter, red)) {
+    gather_partials<3>(a.part, a.counter, tot, red);
     if (threadIdx.x == 0) {
       CgScalars* s = a.sc;
       const double dn = sqrt(fmax(0.0, tot[0]));
@@ -409,7 +460,7 @@ __global__ void k_cg_trials(CgArgs a, int i0, int i1, int last_chunk) {
     __syncwarp();
   }
   if (publish_partials<2 * NT>(acc, a.part, a.counter, red)) {
-    gather_partials<2 * NT>(a.part, a.counter, tot);
+    gather_partials<2 * NT>(a.part, a.counter, tot, red);
     if (threadIdx.x == 0) {
       CgScalars* s = a.sc;
       const double Tm = fmax(a.T_r, 1e-14);
@@ -482,7 +533,10 @@ __global__ void k_cg_step_end(CgArgs a, double phase_rel) {
   } else {
     enc = s->dE > tol;
   }
-  const bool nc = a.tol_grad > 0.0 ? s->grad_norm > a.tol_grad : enc;
+  // FP32 phase: leave it at the energy plateau of the raised tolerance or once the
+  // gradient target is met; FP64 (and the plain solver): the reference rule.
+  const bool nc = phase_rel > 0.0 ? (enc && !(a.tol_grad > 0.0 && s->grad_norm <= a.tol_grad))
+                                  : (a.tol_grad > 0.0 ? s->grad_norm > a.tol_grad : enc);
   s->active = (kn < a.max_iter && nc) ? 1 : 0;
 }
 
@@ -493,9 +547,17 @@ __global__ void k_cg_rearm(CgArgs a) {
   s->active = s->k < a.max_iter ? 1 : 0;
 }
 
-__global__ void k_cg_converged(CgArgs a) {
+__global__ void k_cg_converged(CgArgs a, int switched_at, double* __restrict__ out) {
   CgScalars* s = a.sc;
   s->converged = a.tol_grad > 0.0 ? (s->grad_norm <= a.tol_grad) : (s->k < a.max_iter);
+  out[0] = s->mu;
+  out[1] = s->E_fin;
+  out[2] = (double)s->k;
+  out[3] = (double)s->converged;
+  out[4] = s->grad_norm;
+  out[5] = (double)switched_at;
+  out[6] = 0.0;
+  out[7] = 0.0;
 }
 
 // ============================================================ host driver ===
@@ -546,10 +608,7 @@ struct CgRun {
 
 static size_t smem_eig(int nb) { return (jacobi_smem_elems(nb) + 2 * (size_t)nb * nb) * sizeof(double2) * kSolverWarps; }
 
-static int set_smem(const void* fn, size_t bytes) {
-  HF_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-  return HF_OK;
-}
+static int set_smem(const void* fn, size_t) { return allow_max_dynamic_smem(fn); }
 
 static int cg_fock(CgRun& r, cudaStream_t s, bool fp32, const int* active) {
   const hf_cg_problem& pb = *r.pb;
@@ -580,7 +639,75 @@ static int cg_mu(CgRun& r, cudaStream_t s, int maxiter, const int* active) {
                           maxiter, &r.a.sc->mu, &r.a.sc->mu, active);
 }
 
+// One iteration on the lane-per-row kernels (nb <= 8).
+template <int NB>
+static int cg_iteration_rows(CgRun& r, cudaStream_t s, const hf_cg_config& cf, bool fp32) {
+  const int* act = &r.a.sc->active;
+  const int rb = row_blocks(r.a.nk, RowGroup<NB>::KPW);
+  const int eb = perk_blocks(r.a.nk);
+  k_cgr_density<NB><<<rb, 32 * kRowWarps, 0, s>>>(r.a, 0);
+  HF_LAUNCH_CHECK("k_cgr_density");
+  int st = cg_project(r, s);
+  if (st) return st;
+  if ((st = cg_fock(r, s, fp32, act))) return st;
+  if ((st = cg_energy(r, s, &r.a.sc->E, act))) return st;
+  k_cgr_grad1<NB><<<rb, 32 * kRowWarps, 0, s>>>(r.a);
+  HF_LAUNCH_CHECK("k_cgr_grad1");
+  k_cg_grad2<<<eb, 256, 0, s>>>(r.a);
+  HF_LAUNCH_CHECK("k_cg_grad2");
+  k_cg_dir_lu<<<eb, 256, 0, s>>>(r.a);
+  HF_LAUNCH_CHECK("k_cg_dir_lu");
+  const int bt = cf.bt_max;
+  if (bt >= 1) {
+    k_cgr_trials<NB, 1><<<rb, 32 * kRowWarps, 0, s>>>(r.a, 0, 1, bt == 1);
+    HF_LAUNCH_CHECK("k_cgr_trials");
+    for (int i0 = 1; i0 < bt; i0 += 8) {
+      const int i1 = i0 + 8 < bt ? i0 + 8 : bt;
+      k_cgr_trials<NB, 8><<<rb, 32 * kRowWarps, 0, s>>>(r.a, i0, i1, i1 == bt);
+      HF_LAUNCH_CHECK("k_cgr_trials");
+    }
+  }
+  k_cgr_update<NB><<<rb, 32 * kRowWarps, 0, s>>>(r.a);
+  HF_LAUNCH_CHECK("k_cgr_update");
+  if ((st = cg_mu(r, s, cf.mu_maxiter, act))) return st;
+  k_cg_step_end<<<1, 1, 0, s>>>(r.a, fp32 ? cf.fp32_switch_rel : 0.0);
+  HF_LAUNCH_CHECK("k_cg_step_end");
+  return HF_OK;
+}
+
+template <int NB>
+static int cg_density_rows(CgRun& r, cudaStream_t s, int force) {
+  k_cgr_density<NB><<<row_blocks(r.a.nk, RowGroup<NB>::KPW), 32 * kRowWarps, 0, s>>>(r.a, force);
+  HF_LAUNCH_CHECK("k_cgr_density");
+  return HF_OK;
+}
+
+static int cg_density(CgRun& r, cudaStream_t s, int force) {
+  switch (r.a.nb) {
+#define HF_NB_CASE(N) case N: return cg_density_rows<N>(r, s, force);
+    HF_NB_CASE(1) HF_NB_CASE(2) HF_NB_CASE(3) HF_NB_CASE(4) HF_NB_CASE(5) HF_NB_CASE(6) HF_NB_CASE(7) HF_NB_CASE(8)
+#undef HF_NB_CASE
+    default: break;
+  }
+  const int nb = r.a.nb, nb2 = nb * nb;
+  k_cg_density<<<r.nblk, 32 * kSolverWarps, (2 * (size_t)nb2 + nb) * 16 * kSolverWarps, s>>>(r.a, force);
+  HF_LAUNCH_CHECK("k_cg_density");
+  return HF_OK;
+}
+
+static int cg_iteration_warp(CgRun& r, cudaStream_t s, const hf_cg_config& cf, bool fp32);
+
 static int cg_iteration(CgRun& r, cudaStream_t s, const hf_cg_config& cf, bool fp32) {
+  switch (r.a.nb) {
+#define HF_NB_CASE(N) case N: return cg_iteration_rows<N>(r, s, cf, fp32);
+    HF_NB_CASE(1) HF_NB_CASE(2) HF_NB_CASE(3) HF_NB_CASE(4) HF_NB_CASE(5) HF_NB_CASE(6) HF_NB_CASE(7) HF_NB_CASE(8)
+#undef HF_NB_CASE
+    default: return cg_iteration_warp(r, s, cf, fp32);
+  }
+}
+
+// One iteration on the warp-per-k kernels (9 <= nb <= 16; spectral Cayley).
+static int cg_iteration_warp(CgRun& r, cudaStream_t s, const hf_cg_config& cf, bool fp32) {
   const double phase_rel = fp32 ? cf.fp32_switch_rel : 0.0;
   const int nb = r.pb->nb, nb2 = nb * nb;
   const int* act = &r.a.sc->active;
@@ -622,6 +749,40 @@ static int cg_iteration(CgRun& r, cudaStream_t s, const hf_cg_config& cf, bool f
   return HF_OK;
 }
 
+// ------------------------------------------------------------ one solve ---
+// A solve as a host-side state machine over one stream: start() enqueues the
+// init and the first chunk of iterations, each chunk ends with an async copy of
+// the device scalars to `hs`; once that copy has landed, advance() enqueues the
+// next chunk, the FP32 -> FP64 switch, or the finalize (which writes
+// scalars_out on the device).  hf_cg_solve drives one of these with blocking
+// waits; hf_cg_solve_batch drives many, one per stream, by polling events.
+struct CgSolver {
+  CgRun r{};
+  CgLayout L{};
+  const hf_cg_problem* pb = nullptr;
+  const hf_cg_config* cf = nullptr;
+  cudaStream_t s = nullptr;
+  double* scalars_out = nullptr;
+  CgScalars* hs = nullptr;
+  bool graphs = false, fp32 = false, finalizing = false;
+  int switched_at = -1, chunk = 4;
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+
+  int setup(const hf_cg_problem* pb_, const hf_cg_config* cf_, void* Q, void* p, void* density, void* fock,
+            double* hist_E, double* hist_grad, double* scalars_out_, void* workspace, cudaStream_t s_,
+            CgScalars* host_slot);
+  int start(const void* P0);
+  int launch_chunk();
+  int advance(bool* finished);
+  int launch_finalize();
+  int get_exec(bool f32, cudaGraphExec_t* out);
+  void release() {
+    for (auto& e : exec)
+      if (e) { cudaGraphExecDestroy(e); e = nullptr; }
+  }
+  ~CgSolver() { release(); }
+};
+
 static int cg_check(const hf_cg_problem* pb, const hf_cg_config* cf) {
   if (!pb || !cf) return fail(HF_ERR_INVALID, "NULL problem/config");
   if (pb->nk1 < 1 || pb->nk2 < 1 || pb->nb < 1) return fail(HF_ERR_INVALID, "bad shape");
@@ -647,26 +808,23 @@ extern "C" int hf_cg_workspace_size(const hf_cg_problem* pb, const hf_cg_config*
   return HF_OK;
 }
 
-extern "C" int hf_cg_solve(void* stream, const hf_cg_problem* pb, const hf_cg_config* cf, const void* P0,
-                           void* Q, void* p, void* density, void* fock, double* hist_E, double* hist_grad,
-                           double* scalars_out, void* workspace, size_t workspace_bytes) {
-  int st = cg_check(pb, cf);
-  if (st) return st;
-  if (!P0 || !Q || !p || !density || !fock || !scalars_out || !workspace)
-    return fail(HF_ERR_INVALID, "NULL argument");
-  size_t need = 0;
-  if ((st = hf_cg_workspace_size(pb, cf, &need))) return st;
-  if (workspace_bytes < need) return fail(HF_ERR_WORKSPACE, "CG workspace too small: need " + std::to_string(need));
+namespace hf {
+
+int CgSolver::setup(const hf_cg_problem* pb_, const hf_cg_config* cf_, void* Q, void* p, void* density,
+                    void* fock, double* hist_E, double* hist_grad, double* scalars_out_, void* workspace,
+                    cudaStream_t s_, CgScalars* host_slot) {
+  pb = pb_;
+  cf = cf_;
+  s = s_;
+  hs = host_slot;
+  scalars_out = scalars_out_;
   size_t fws = 0, f2 = 0, rws = 0;
-  fock_ws_size(*pb, fock_flags(*pb, false), &fws);
-  fock_ws_size(*pb, fock_flags(*pb, true), &f2);
-  hf_reduce_workspace_size(pb->nk1, pb->nk2, pb->nb, &rws);
-  CgLayout L;
+  int st;
+  if ((st = fock_ws_size(*pb, fock_flags(*pb, false), &fws))) return st;
+  if ((st = fock_ws_size(*pb, fock_flags(*pb, true), &f2))) return st;
+  if ((st = hf_reduce_workspace_size(pb->nk1, pb->nk2, pb->nb, &rws))) return st;
   cg_layout(*pb, fws > f2 ? fws : f2, rws, L);
   char* ws = static_cast<char*>(workspace);
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-
-  CgRun r;
   r.pb = pb;
   r.cf = cf;
   CgArgs& a = r.a;
@@ -712,13 +870,21 @@ extern "C" int hf_cg_solve(void* stream, const hf_cg_problem* pb, const hf_cg_co
   a.hist_E = hist_E ? hist_E : reinterpret_cast<double*>(ws + L.total);
   a.hist_G = hist_grad ? hist_grad : reinterpret_cast<double*>(ws + L.total) + cf->max_iter;
   r.nblk = perk_blocks(a.nk);
-
+  fp32 = cf->fp32_exchange != 0;
+  chunk = cf->chunk > 0 ? cf->chunk : 4;
+  graphs = cf->fock_cb == nullptr && cf->project_cb == nullptr && s != nullptr;
   const int nb = pb->nb, nb2 = nb * nb;
   if ((st = set_smem((const void*)k_cg_eig, smem_eig(nb)))) return st;
   if ((st = set_smem((const void*)k_cg_dir, smem_eig(nb)))) return st;
   if ((st = set_smem((const void*)k_cg_update, (4 * (size_t)nb2 + nb) * 16 * kSolverWarps))) return st;
   if ((st = set_smem((const void*)k_cg_grad1, 3 * (size_t)nb2 * 16 * kSolverWarps))) return st;
+  return HF_OK;
+}
 
+int CgSolver::start(const void* P0) {
+  CgArgs& a = r.a;
+  const int nb = pb->nb, nb2 = nb * nb;
+  int st;
   HF_CUDA(cudaMemsetAsync(r.H, 0, sizeof(double2) * nb2, s));  // H stays zero without Hartree
   if (cf->max_iter > 0) HF_CUDA(cudaMemsetAsync(a.hist_E, 0, sizeof(double) * cf->max_iter, s));
   if (cf->max_iter > 0) HF_CUDA(cudaMemsetAsync(a.hist_G, 0, sizeof(double) * cf->max_iter, s));
@@ -726,59 +892,277 @@ extern "C" int hf_cg_solve(void* stream, const hf_cg_problem* pb, const hf_cg_co
   k_cg_init<<<r.nblk, 256, 0, s>>>(a, static_cast<const double2*>(P0), static_cast<const double*>(pb->w2d),
                                    pb->weight_sum);
   HF_LAUNCH_CHECK("k_cg_init");
-  const bool mixed = cf->fp32_exchange != 0;
   if ((st = cg_fock(r, s, false, nullptr))) return st;
   k_cg_eig<<<r.nblk, 32 * kSolverWarps, smem_eig(nb), s>>>(a, a.F, 0);
   HF_LAUNCH_CHECK("k_cg_eig");
   if ((st = cg_mu(r, s, cf->mu_maxiter, nullptr))) return st;
+  return cf->max_iter > 0 ? launch_chunk() : launch_finalize();
+}
 
-  // ---- loop (solver.py:603-604), chunks of iterations between host checks ----
-  int host_k = 0, host_active = cf->max_iter > 0;
-  bool fp32 = mixed;
-  int switched_at = -1;
-  const int chunk = cf->chunk > 0 ? cf->chunk : 4;
-  CgScalars hs;
-  while (host_active) {
+// One iteration captured into a CUDA graph per precision phase (no host
+// callbacks); every kernel of it returns at once once the device stop flag is
+// clear, so a chunk may overrun convergence at no cost.
+int CgSolver::get_exec(bool f32, cudaGraphExec_t* out) {
+  cudaGraphExec_t& e = exec[f32 ? 1 : 0];
+  if (!e) {
+    cudaGraph_t g = nullptr;
+    HF_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    const int st2 = cg_iteration(r, s, *cf, f32);
+    const cudaError_t ce = cudaStreamEndCapture(s, &g);
+    if (st2 != HF_OK) {
+      if (g) cudaGraphDestroy(g);
+      return st2;
+    }
+    if (ce != cudaSuccess) return cuda_check(ce, "cudaStreamEndCapture");
+    const cudaError_t ie = cudaGraphInstantiate(&e, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) return cuda_check(ie, "cudaGraphInstantiate");
+  }
+  *out = e;
+  return HF_OK;
+}
+
+// ---- loop (solver.py:603-604): `chunk` iterations, then the scalars to the host ----
+int CgSolver::launch_chunk() {
+  int st;
+  if (graphs) {
+    cudaGraphExec_t e = nullptr;
+    if ((st = get_exec(fp32, &e))) return st;
+    for (int c = 0; c < chunk; ++c) HF_CUDA(cudaGraphLaunch(e, s));
+  } else {
     for (int c = 0; c < chunk; ++c)
       if ((st = cg_iteration(r, s, *cf, fp32))) return st;
-    HF_CUDA(cudaMemcpyAsync(&hs, a.sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, s));
-    HF_CUDA(cudaStreamSynchronize(s));
-    host_k = hs.k;
-    host_active = hs.active;
-    if (!std::isfinite(hs.E)) break;
+  }
+  HF_CUDA(cudaMemcpyAsync(hs, r.a.sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, s));
+  return HF_OK;
+}
+
+int CgSolver::advance(bool* finished) {
+  *finished = false;
+  if (finalizing) {
+    *finished = true;
+    return HF_OK;
+  }
+  const int host_k = hs->k;
+  int host_active = hs->active;
+  if (!std::isfinite(hs->E)) {
+    host_active = 0;
+  } else if (fp32 && host_k < cf->max_iter && (!host_active || host_k >= cf->max_iter / 2)) {
     // mixed precision: FP32 exchange until the windowed energy change reaches the FP32
     // noise floor (or half the iteration budget), then FP64 defect-correction builds
     // continue from the same state to the requested tolerance.
-    if (fp32 && host_k < cf->max_iter && (!host_active || host_k >= cf->max_iter / 2)) {
-      fp32 = false;
-      switched_at = host_k;
-      k_cg_rearm<<<1, 1, 0, s>>>(a);
-      HF_LAUNCH_CHECK("k_cg_rearm");
-      host_active = 1;
-    }
+    fp32 = false;
+    switched_at = host_k;
+    k_cg_rearm<<<1, 1, 0, s>>>(r.a);
+    HF_LAUNCH_CHECK("k_cg_rearm");
+    host_active = 1;
   }
-  (void)host_k;
+  return host_active ? launch_chunk() : launch_finalize();
+}
 
-  // ---- finalize (solver.py:613-648) ----
-  k_cg_density<<<r.nblk, 32 * kSolverWarps, (2 * (size_t)nb2 + nb) * 16 * kSolverWarps, s>>>(a, 1);
-  HF_LAUNCH_CHECK("k_cg_density");
+// ---- finalize (solver.py:613-648) ----
+int CgSolver::launch_finalize() {
+  CgArgs& a = r.a;
+  const int nb = pb->nb, nb2 = nb * nb;
+  int st;
+  finalizing = true;
+  if ((st = cg_density(r, s, 1))) return st;
   if ((st = cg_project(r, s))) return st;
   if ((st = cg_fock(r, s, false, nullptr))) return st;
   k_cg_eig<<<r.nblk, 32 * kSolverWarps, smem_eig(nb), s>>>(a, a.F, 1);
   HF_LAUNCH_CHECK("k_cg_eig");
   if ((st = cg_mu(r, s, cf->mu_maxiter, nullptr))) return st;
-  k_cg_density<<<r.nblk, 32 * kSolverWarps, (2 * (size_t)nb2 + nb) * 16 * kSolverWarps, s>>>(a, 1);
-  HF_LAUNCH_CHECK("k_cg_density");
+  if ((st = cg_density(r, s, 1))) return st;
   if ((st = cg_project(r, s))) return st;
   if ((st = cg_fock(r, s, false, nullptr))) return st;
   if ((st = cg_energy(r, s, &a.sc->E_fin, nullptr))) return st;
-  k_cg_converged<<<1, 1, 0, s>>>(a);
+  k_cg_converged<<<1, 1, 0, s>>>(a, switched_at, scalars_out);
   HF_LAUNCH_CHECK("k_cg_converged");
-  HF_CUDA(cudaMemcpyAsync(&hs, a.sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, s));
-  HF_CUDA(cudaStreamSynchronize(s));
-  const double out[8] = {hs.mu, hs.E_fin, (double)hs.k, (double)hs.converged, hs.grad_norm,
-                         (double)switched_at, 0.0, 0.0};
-  HF_CUDA(cudaMemcpyAsync(scalars_out, out, sizeof(out), cudaMemcpyHostToDevice, s));
-  HF_CUDA(cudaStreamSynchronize(s));
+  HF_CUDA(cudaMemcpyAsync(hs, a.sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, s));
   return HF_OK;
+}
+
+// A non-blocking stream that starts after `user` and that `user` waits for at
+// the end (legacy default streams cannot be captured).
+struct LaneStream {
+  cudaStream_t s = nullptr;
+  cudaEvent_t ev = nullptr;
+  int open(cudaStream_t user) {
+    HF_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    HF_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    HF_CUDA(cudaEventRecord(ev, user));
+    HF_CUDA(cudaStreamWaitEvent(s, ev, 0));
+    return HF_OK;
+  }
+  int join(cudaStream_t user) {
+    HF_CUDA(cudaEventRecord(ev, s));
+    HF_CUDA(cudaStreamWaitEvent(user, ev, 0));
+    return HF_OK;
+  }
+  ~LaneStream() {
+    if (s) {
+      cudaStreamSynchronize(s);
+      cudaStreamDestroy(s);
+    }
+    if (ev) cudaEventDestroy(ev);
+  }
+};
+
+}  // namespace hf
+
+extern "C" int hf_cg_solve(void* stream, const hf_cg_problem* pb, const hf_cg_config* cf, const void* P0,
+                           void* Q, void* p, void* density, void* fock, double* hist_E, double* hist_grad,
+                           double* scalars_out, void* workspace, size_t workspace_bytes) {
+  int st = cg_check(pb, cf);
+  if (st) return st;
+  if (!P0 || !Q || !p || !density || !fock || !scalars_out || !workspace)
+    return fail(HF_ERR_INVALID, "NULL argument");
+  size_t need = 0;
+  if ((st = hf_cg_workspace_size(pb, cf, &need))) return st;
+  if (workspace_bytes < need) return fail(HF_ERR_WORKSPACE, "CG workspace too small: need " + std::to_string(need));
+  cudaStream_t user = static_cast<cudaStream_t>(stream);
+  // host callbacks enqueue on the caller's stream; otherwise a private stream
+  // (capturable) ordered after it
+  const bool callbacks = cf->fock_cb != nullptr || cf->project_cb != nullptr;
+  LaneStream lane;
+  if (!callbacks && (st = lane.open(user))) return st;
+  const cudaStream_t s = callbacks ? user : lane.s;
+  CgScalars hs{};
+  CgSolver sv;
+  if ((st = sv.setup(pb, cf, Q, p, density, fock, hist_E, hist_grad, scalars_out, workspace, s, &hs))) return st;
+  if ((st = sv.start(P0))) return st;
+  bool finished = false;
+  while (!finished) {
+    HF_CUDA(cudaStreamSynchronize(s));
+    if ((st = sv.advance(&finished))) return st;
+  }
+  return callbacks ? HF_OK : lane.join(user);
+}
+
+extern "C" int hf_cg_batch_workspace_size(const hf_cg_batch_item* items, int n_items, const hf_cg_config* cf,
+                                          size_t* bytes_per_lane) {
+  if (!items || n_items < 1 || !cf || !bytes_per_lane) return fail(HF_ERR_INVALID, "bad batch arguments");
+  size_t mx = 0;
+  for (int i = 0; i < n_items; ++i) {
+    size_t b = 0;
+    const int st = hf_cg_workspace_size(&items[i].problem, cf, &b);
+    if (st) return st;
+    mx = b > mx ? b : mx;
+  }
+  *bytes_per_lane = align_up(mx, 256);  // every lane's workspace starts 256-byte aligned
+  return HF_OK;
+}
+
+extern "C" int hf_cg_solve_batch(void* stream, const hf_cg_batch_item* items, int n_items, const hf_cg_config* cf,
+                                 int n_lanes, void* workspace, size_t bytes_per_lane, double* solve_ms) {
+  if (!items || n_items < 1 || !cf || !workspace || n_lanes < 1) return fail(HF_ERR_INVALID, "bad batch arguments");
+  if (cf->fock_cb || cf->project_cb) return fail(HF_ERR_INVALID, "the batched CG driver takes no host callbacks");
+  size_t need = 0;
+  int st = hf_cg_batch_workspace_size(items, n_items, cf, &need);
+  if (st) return st;
+  if (bytes_per_lane < need) return fail(HF_ERR_WORKSPACE, "CG batch workspace too small: need " + std::to_string(need) + " per lane");
+  for (int i = 0; i < n_items; ++i) {
+    const hf_cg_batch_item& it = items[i];
+    if (!it.P0 || !it.Q || !it.p || !it.density || !it.fock || !it.scalars_out)
+      return fail(HF_ERR_INVALID, "NULL argument in batch item " + std::to_string(i));
+  }
+  if (n_lanes > n_items) n_lanes = n_items;
+  cudaStream_t user = static_cast<cudaStream_t>(stream);
+
+  // longest first (per-k work ~ nk nb^3, FFT ~ nk nb^2 log nk): a greedy list schedule
+  std::vector<int> order(n_items);
+  for (int i = 0; i < n_items; ++i) order[i] = i;
+  auto cost = [&](int i) {
+    const hf_cg_problem& q = items[i].problem;
+    return (double)q.nk1 * q.nk2 * q.nb * q.nb * (q.nb + 8.0);
+  };
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost(x) > cost(y); });
+
+  CgScalars* hslots = nullptr;
+  HF_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&hslots), sizeof(CgScalars) * n_lanes, cudaHostAllocDefault));
+  struct Lane {
+    LaneStream ls;
+    cudaEvent_t ready = nullptr, t0 = nullptr, t1 = nullptr;
+    CgSolver* sv = nullptr;
+    int item = -1;
+  };
+  std::vector<Lane> lanes(n_lanes);
+  auto cleanup = [&]() {
+    for (auto& l : lanes) {
+      if (l.ls.s) cudaStreamSynchronize(l.ls.s);
+      delete l.sv;
+      l.sv = nullptr;
+      if (l.ready) cudaEventDestroy(l.ready);
+      if (l.t0) cudaEventDestroy(l.t0);
+      if (l.t1) cudaEventDestroy(l.t1);
+      l.ready = l.t0 = l.t1 = nullptr;
+    }
+    cudaFreeHost(hslots);
+  };
+  auto run = [&]() -> int {
+    for (auto& l : lanes) {
+      int e;
+      if ((e = l.ls.open(user))) return e;
+      HF_CUDA(cudaEventCreateWithFlags(&l.ready, cudaEventDisableTiming));
+      HF_CUDA(cudaEventCreate(&l.t0));
+      HF_CUDA(cudaEventCreate(&l.t1));
+    }
+    int next = 0, busy = 0;
+    for (;;) {
+      bool progressed = false;
+      for (int li = 0; li < n_lanes; ++li) {
+        Lane& l = lanes[li];
+        char* ws = static_cast<char*>(workspace) + (size_t)li * bytes_per_lane;
+        if (!l.sv) {
+          if (next >= n_items) continue;
+          const int i = order[next++];
+          const hf_cg_batch_item& it = items[i];
+          l.sv = new CgSolver();
+          l.item = i;
+          int e;
+          if ((e = l.sv->setup(&it.problem, cf, it.Q, it.p, it.density, it.fock, it.hist_E, it.hist_grad,
+                               it.scalars_out, ws, l.ls.s, &hslots[li])))
+            return e;
+          HF_CUDA(cudaEventRecord(l.t0, l.ls.s));
+          if ((e = l.sv->start(it.P0))) return e;
+          HF_CUDA(cudaEventRecord(l.ready, l.ls.s));
+          ++busy;
+          progressed = true;
+          continue;
+        }
+        const cudaError_t q = cudaEventQuery(l.ready);
+        if (q == cudaErrorNotReady) continue;
+        if (q != cudaSuccess) return cuda_check(q, "cudaEventQuery");
+        bool finished = false;
+        int e;
+        if ((e = l.sv->advance(&finished))) return e;
+        if (finished) {
+          HF_CUDA(cudaEventRecord(l.t1, l.ls.s));
+          if (solve_ms) {
+            HF_CUDA(cudaEventSynchronize(l.t1));
+            float ms = 0.f;
+            HF_CUDA(cudaEventElapsedTime(&ms, l.t0, l.t1));
+            solve_ms[l.item] = ms;
+          }
+          delete l.sv;
+          l.sv = nullptr;
+          l.item = -1;
+          --busy;
+        } else {
+          HF_CUDA(cudaEventRecord(l.ready, l.ls.s));
+        }
+        progressed = true;
+      }
+      if (busy == 0 && next >= n_items) break;
+      if (!progressed) std::this_thread::yield();
+    }
+    for (auto& l : lanes) {
+      int e;
+      if ((e = l.ls.join(user))) return e;
+    }
+    return HF_OK;
+  };
+  st = run();
+  cleanup();
+  return st;
 }

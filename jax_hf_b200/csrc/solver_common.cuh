@@ -33,17 +33,24 @@ __device__ __forceinline__ bool publish_partials(KSum (&acc)[NS], double* __rest
   return s_last;
 }
 
-// In the last CTA: totals[q] = sum over blocks (thread q sums in block order).
+// In the last CTA: totals[q] = sum over blocks.  Every thread sums a fixed
+// strided subset of the block partials, then one compensated block reduction per
+// quantity (fixed assignment and tree -> deterministic for a launch shape).
 template <int NS>
 __device__ __forceinline__ void gather_partials(const double* __restrict__ part, unsigned* __restrict__ counter,
-                                                double* totals) {
-  if (threadIdx.x < NS) {
-    KSum t;
-    for (unsigned b = 0; b < gridDim.x; ++b) {
-      t.add(__ldcg(part + ((size_t)b * NS + threadIdx.x) * 2));
-      t.add(__ldcg(part + ((size_t)b * NS + threadIdx.x) * 2 + 1));
+                                                double* totals, double* sm) {
+  KSum t[NS];
+  for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+#pragma unroll
+    for (int q = 0; q < NS; ++q) {
+      t[q].add(__ldcg(part + ((size_t)b * NS + q) * 2));
+      t[q].add(__ldcg(part + ((size_t)b * NS + q) * 2 + 1));
     }
-    totals[threadIdx.x] = t.value();
+  }
+#pragma unroll
+  for (int q = 0; q < NS; ++q) {
+    const KSum r = block_reduce(t[q], sm);
+    if (threadIdx.x == 0) totals[q] = r.value();
   }
   __syncthreads();
   if (threadIdx.x == 0) *counter = 0u;

@@ -254,3 +254,71 @@ def solve_direct_minimization(kernel, P0, n_electrons: float, *, config: SolverC
 
 
 solve = solve_direct_minimization
+
+
+class _CgBatchItem(C.Structure):
+    _fields_ = [("problem", _CgProblem), ("P0", C.c_void_p), ("Q", C.c_void_p), ("p", C.c_void_p),
+                ("density", C.c_void_p), ("fock", C.c_void_p), ("hist_E", C.c_void_p), ("hist_grad", C.c_void_p),
+                ("scalars_out", C.c_void_p)]
+
+
+def solve_batch(kernels, P0s, n_electrons, *, config: SolverConfig | None = None, lanes: int = 8,
+                return_times: bool = False):
+    """Many independent CG solves in one native call (density scans).
+
+    ``kernels``, ``P0s`` and ``n_electrons`` are equal-length sequences; each
+    solve has the semantics of ``solve(kernel, P0, n, config=config)`` with
+    ``optimizer="cg"`` and no hooks.  The C driver runs ``lanes`` solves at a
+    time, each on its own stream with CUDA-graph iterations, longest first.
+    Returns the list of ``SolveResult`` (and, with ``return_times``, each
+    solve's device time in ms from its start to its final scalars).
+    """
+    cfg = config or SolverConfig()
+    if str(cfg.optimizer).lower() != "cg":
+        raise ValueError("solve_batch runs the CG optimizer only.")
+    if cfg.project_fn is not None or cfg.block_sizes is not None or cfg.deflation_targets is not None:
+        raise ValueError("solve_batch takes no project_fn, block_sizes or deflation hooks.")
+    n = len(kernels)
+    if n == 0 or len(P0s) != n or len(n_electrons) != n:
+        raise ValueError("kernels, P0s and n_electrons must be non-empty and of equal length.")
+    L = _lib.lib()
+    dev = kernels[0].device
+    conf = _CgConfig(int(cfg.max_iter), float(cfg.tol_E), float(cfg.tol_grad), float(cfg.denom_scale),
+                     float(cfg.max_step), int(cfg.cg_restart), float(cfg.bt_shrink), int(cfg.bt_max),
+                     int(cfg.mu_maxiter), int(cfg.plateau_window), int(bool(cfg.fp32_exchange)),
+                     float(cfg.fp32_switch_rel), int(cfg.chunk), FOCK_CB(), PROJECT_CB(), None)
+    items = (_CgBatchItem * n)()
+    keep, outs = [], []
+    for i, (kern, P0, ne) in enumerate(zip(kernels, P0s, n_electrons)):
+        validate_electron_count(kern.w2d, kern.h.shape[-1], ne, context="n_electrons")
+        nk1, nk2, nb = kern.shape
+        kc = KernelC128(kern)
+        P0t = torch.as_tensor(P0).to(dev, torch.complex128).contiguous()
+        Q = torch.empty((nk1, nk2, nb, nb), dtype=torch.complex128, device=dev)
+        p = torch.empty((nk1, nk2, nb), dtype=torch.float64, device=dev)
+        P, F = torch.empty_like(Q), torch.empty_like(Q)
+        hE = torch.zeros(max(cfg.max_iter, 1), dtype=torch.float64, device=dev)
+        hG = torch.zeros(max(cfg.max_iter, 1), dtype=torch.float64, device=dev)
+        sc = torch.zeros(8, dtype=torch.float64, device=dev)
+        items[i] = _CgBatchItem(kc.problem(ne), P0t.data_ptr(), Q.data_ptr(), p.data_ptr(), P.data_ptr(),
+                                F.data_ptr(), hE.data_ptr(), hG.data_ptr(), sc.data_ptr())
+        keep += [kc, P0t]
+        outs.append((kern, Q, p, P, F, hE, hG, sc))
+    per_lane = C.c_size_t(0)
+    _lib.check(L.hf_cg_batch_workspace_size(items, n, C.byref(conf), C.byref(per_lane)))
+    lanes = max(1, min(int(lanes), n))
+    ws = torch.empty(lanes * per_lane.value, dtype=torch.uint8, device=dev)
+    times = (C.c_double * n)()
+    _lib.check(L.hf_cg_solve_batch(_lib.stream_ptr(dev), items, n, C.byref(conf), lanes, ws.data_ptr(),
+                                   per_lane.value, times))
+    results = []
+    for kern, Q, p, P, F, hE, hG, sc in outs:
+        s = sc.cpu().numpy()
+        hist = dict(E=hE[:cfg.max_iter].to(kern.real_dtype), grad_norm=hG[:cfg.max_iter].to(kern.real_dtype),
+                    fp32_switch_iter=int(s[5]))
+        results.append(SolveResult(Q=Q.to(kern.dtype), p=p.to(kern.real_dtype), mu=sc[0].to(kern.real_dtype),
+                                   density=P.to(kern.dtype), fock=F.to(kern.dtype), energy=sc[1].clone(),
+                                   n_iter=torch.tensor(int(s[2]), dtype=torch.int32),
+                                   converged=torch.tensor(bool(s[3])), history=hist))
+    del keep
+    return (results, list(times)) if return_times else results

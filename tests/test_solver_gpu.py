@@ -57,6 +57,8 @@ CASES = [
     ("fourier_12_nb4_scalar", _fourier(12, 4, "scalar", 0.1, 3), 2.0, dict(max_iter=200, tol_E=1e-10)),
     ("fourier_10_nb3_layer", _fourier(10, 3, "layer", 0.05, 4), 1.3, dict(max_iter=200, tol_E=1e-10)),
     ("contact_k2", _contact(), 4.0, dict(max_iter=200, tol_E=1e-10)),
+    ("fourier_8_nb8_layer", _fourier(8, 8, "layer", 0.1, 6), 3.0, dict(max_iter=200, tol_E=1e-10)),
+    ("fourier_6_nb10_scalar_warp_path", _fourier(6, 10, "scalar", 0.1, 5), 5.0, dict(max_iter=200, tol_E=1e-10)),
     ("gradstop_dirac_k4", _dirac(), 16.0, dict(max_iter=300, tol_grad=1e-6)),
 ]
 
@@ -122,3 +124,56 @@ def test_cg_rejects_unreachable_count(cuda):
     K = G.HartreeFockKernel(**_two_band())
     with pytest.raises(ValueError, match="physically reachable range"):
         solve(K, torch.zeros((1, 1, 2, 2), dtype=torch.complex128, device="cuda"), 3.0)
+
+
+def _scan_problems():
+    out = []
+    for i, (nk, nb, V) in enumerate(((12, 4, "scalar"), (16, 6, "layer"), (24, 4, "layer"), (12, 8, "scalar"),
+                                     (18, 3, "scalar"))):
+        out.append(S.fourier_problem(nk, nb, 2.0, seed=70 + i, V=V, T=0.1, n_electrons=(0.2 + 0.15 * i) * nb))
+    return out
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_cg_batch_matches_single_solves(cuda, mixed):
+    """hf_cg_solve_batch: every solve of the batch equals the same solve run alone (same kernels, same order)."""
+    import jax_hf_b200 as G
+    from jax_hf_b200.solver import SolverConfig, solve, solve_batch
+    probs = _scan_problems()
+    cfg = SolverConfig(max_iter=150, tol_E=1e-10, fp32_exchange=mixed)
+    Ks = [G.HartreeFockKernel(**p.kernel_kwargs()) for p in probs]
+    P0s = [np.zeros((p.nk, p.nk, p.nb, p.nb), complex) for p in probs]
+    res, times = solve_batch(Ks, P0s, [p.n_electrons for p in probs], config=cfg, lanes=3, return_times=True)
+    assert len(res) == len(probs) and all(t > 0 for t in times)
+    for K, P0, p, r in zip(Ks, P0s, probs, res):
+        r1 = solve(K, torch.as_tensor(P0, device="cuda"), p.n_electrons, config=cfg)
+        assert int(r.n_iter) == int(r1.n_iter)
+        assert bool(r.converged) == bool(r1.converged)
+        assert abs(float(r.energy) - float(r1.energy)) <= 1e-12 * max(1.0, abs(float(r1.energy)))
+        assert torch.allclose(r.density, r1.density, atol=1e-12, rtol=0)
+        assert r.history["fp32_switch_iter"] == r1.history["fp32_switch_iter"]
+
+
+def test_cg_batch_matches_oracle(cuda):
+    """Batched FP64 solves against the oracle's CG on the same inputs."""
+    import jax_hf_b200 as G
+    from jax_hf_b200.solver import SolverConfig, solve_batch
+    probs = _scan_problems()[:3]
+    cfg = dict(max_iter=150, tol_E=1e-10)
+    Ks = [G.HartreeFockKernel(**p.kernel_kwargs()) for p in probs]
+    P0s = [np.zeros((p.nk, p.nk, p.nb, p.nb), complex) for p in probs]
+    res = solve_batch(Ks, P0s, [p.n_electrons for p in probs], config=SolverConfig(**cfg), lanes=2)
+    for p, P0, r in zip(probs, P0s, res):
+        ro = O.solve(O.Kernel(**p.kernel_kwargs()), P0, p.n_electrons, config=O.SolverConfig(**cfg))
+        assert abs(float(r.energy) - ro["energy"]) <= 1e-9 * max(1.0, abs(ro["energy"]))
+        assert np.abs(r.density.cpu().numpy() - ro["density"]).max() < 1e-6
+
+
+def test_cg_batch_rejects_hooks(cuda):
+    import jax_hf_b200 as G
+    from jax_hf_b200.solver import SolverConfig, solve_batch
+    p = _scan_problems()[0]
+    K = G.HartreeFockKernel(**p.kernel_kwargs())
+    with pytest.raises(ValueError, match="hooks"):
+        solve_batch([K], [np.zeros((p.nk, p.nk, p.nb, p.nb), complex)], [p.n_electrons],
+                    config=SolverConfig(block_sizes=(2, 2)))
