@@ -66,7 +66,7 @@ class Clocks:
         self.gpu = gpu_index
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--id={gpu_index}", f"--query-gpu={self.Q}",
-                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                       "--format=csv,noheader,nounits", "-lms", "50"],
                                       stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.p = None
@@ -201,6 +201,9 @@ def run_ours(args, ws, rank, local):
         variants[name] = {"builds_per_s": round(1e6 / us, 1), "us_per_build": round(us, 2),
                           "achieved_gbs": round(nbytes / (us * 1e-6) / 1e9, 1)}
 
+    solves = run_solves(dev) if args.solves else None
+    variants["solves"] = solves
+
     # e2e: public API with host buffers (H2D P from pinned memory, D2H Sigma and F)
     hP = torch.from_numpy(P_np).pin_memory()
     hS = torch.empty(P.shape, dtype=P.dtype).pin_memory()
@@ -232,6 +235,100 @@ def run_ours(args, ws, rank, local):
     nbytes_state = P.numel() * P.element_size()
     return _finish(args, ws, rank, value, dev_ms, avg_us, n_builds, t_wall, clocks, variants, e2e_val,
                    nbytes_state, P_np, prob)
+
+
+def run_solves(dev):
+    """Whole-solve throughput on the solver workloads (device time, CUDA events).
+
+    scf_diis_24x24_nb4: solve_scf (DIIS), FP64.  cg_144x144_nb8: CG at tol_E=1e-9,
+    plain FP64 against mixed (FP32 exchange, FP64 finish).  density_scan_64: the 64
+    solves of the scan (meshes 36..120, nb 4/6/8, CG tol_E=1e-9) solve by solve in
+    FP64, then batched (one native call, 16 streams) in FP64 and mixed; |dE/E| of
+    every batched solve against the same solve's plain FP64 result.
+    """
+    import torch
+    import jax_hf_b200 as G
+    from jax_hf_b200 import synthetic as S
+    from jax_hf_b200.reference_scf import SCFConfig, solve_scf
+    from jax_hf_b200.solver import SolverConfig, solve, solve_batch
+
+    stream = torch.cuda.current_stream()
+
+    def ev_time(fn, reps=1):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        out = None
+        for _ in range(reps):
+            out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return out, e0.elapsed_time(e1) / reps
+
+    out = {}
+    # SCF-DIIS 24x24 nb=4
+    p0 = S.scf_diis_24()
+    K0 = G.HartreeFockKernel(**p0.kernel_kwargs())
+    P00 = torch.zeros((24, 24, 4, 4), dtype=torch.complex128, device=dev)
+    scfg = SCFConfig(acceleration="diis")
+    solve_scf(K0, P00, p0.n_electrons, config=scfg)
+    r0, ms0 = ev_time(lambda: solve_scf(K0, P00, p0.n_electrons, config=scfg), reps=3)
+    out["scf_diis_24x24_nb4_fp64"] = {"solves_per_s": round(1e3 / ms0, 2), "ms_per_solve": round(ms0, 2),
+                                     "iterations": int(r0.iterations), "converged": bool(r0.converged),
+                                     "energy": float(r0.energy)}
+    # CG 144x144 nb=8, FP64 vs mixed
+    p2 = S.cg_144()
+    K2 = G.HartreeFockKernel(**p2.kernel_kwargs())
+    P02 = torch.zeros((144, 144, 8, 8), dtype=torch.complex128, device=dev)
+    res = {}
+    for name, cfg in (("fp64", SolverConfig(max_iter=400, tol_E=1e-9)),
+                      ("mixed", SolverConfig(max_iter=400, tol_E=1e-9, fp32_exchange=True))):
+        solve(K2, P02, p2.n_electrons, config=cfg)
+        r, ms = ev_time(lambda: solve(K2, P02, p2.n_electrons, config=cfg), reps=3)
+        res[name] = (r, ms)
+    E64 = float(res["fp64"][0].energy)
+    cg2 = {}
+    for name, (r, ms) in res.items():
+        cg2[name] = {"solves_per_s": round(1e3 / ms, 2), "ms_per_solve": round(ms, 2), "n_iter": int(r.n_iter),
+                     "converged": bool(r.converged), "energy": float(r.energy),
+                     "rel_dE_vs_fp64": abs(float(r.energy) - E64) / abs(E64),
+                     "max_abs_dP_vs_fp64": float((r.density - res["fp64"][0].density).abs().max())}
+    out["cg_144x144_nb8"] = cg2
+    # density scan: 64 solves
+    probs = S.density_scan(64)
+    Ks = [G.HartreeFockKernel(**p.kernel_kwargs()) for p in probs]
+    P0s = [torch.zeros((p.nk, p.nk, p.nb, p.nb), dtype=torch.complex128, device=dev) for p in probs]
+    nes = [p.n_electrons for p in probs]
+    c64 = SolverConfig(max_iter=400, tol_E=1e-9)
+    cmx = SolverConfig(max_iter=400, tol_E=1e-9, fp32_exchange=True)
+    for K, P0, ne in zip(Ks[:4], P0s[:4], nes[:4]):
+        solve(K, P0, ne, config=c64)
+    solve_batch(Ks, P0s, nes, config=c64, lanes=16)
+    solve_batch(Ks, P0s, nes, config=cmx, lanes=16)
+    t_one, E_one, r_one = [], [], []
+    torch.cuda.synchronize()
+    for K, P0, ne in zip(Ks, P0s, nes):
+        r, ms = ev_time(lambda: solve(K, P0, ne, config=c64))
+        t_one.append(ms)
+        E_one.append(float(r.energy))
+    E_one = np.array(E_one)
+    scan = {"n_solves": len(probs), "tol_E": 1e-9,
+            "fp64_solve_by_solve": {"solves_per_s": round(len(probs) / (sum(t_one) / 1e3), 2),
+                                    "total_ms": round(sum(t_one), 2),
+                                    "p50_ms": round(float(np.percentile(t_one, 50)), 2),
+                                    "p99_ms": round(float(np.percentile(t_one, 99)), 2)}}
+    for name, cfg in (("fp64_batched", c64), ("mixed_batched", cmx)):
+        (rb, tb), ms = ev_time(lambda: solve_batch(Ks, P0s, nes, config=cfg, lanes=16, return_times=True))
+        Eb = np.array([float(r.energy) for r in rb])
+        rel = np.abs(Eb - E_one) / np.abs(E_one)
+        scan[name] = {"solves_per_s": round(len(probs) / (ms / 1e3), 2), "total_ms": round(ms, 2),
+                      "p50_ms": round(float(np.percentile(tb, 50)), 2),
+                      "p99_ms": round(float(np.percentile(tb, 99)), 2), "lanes": 16,
+                      "max_rel_dE_vs_fp64": float(rel.max()), "n_rel_dE_above_1e-9": int((rel > 1e-9).sum()),
+                      "all_converged": bool(all(bool(r.converged) for r in rb)),
+                      "speedup_vs_fp64_solve_by_solve": round(sum(t_one) / ms, 3)}
+    out["density_scan_64"] = scan
+    return out
 
 
 def _finish(args, ws, rank, value, dev_ms, avg_us, n_builds, t_wall, clocks, variants, e2e_val,
@@ -266,6 +363,9 @@ def _finish(args, ws, rank, value, dev_ms, avg_us, n_builds, t_wall, clocks, var
         "gpu_launches": 3 * n_builds,
         "clocks": clocks,
     }
+    solves = variants.pop("solves", None)
+    if solves is not None:
+        line["solves"] = solves
     if args.cpu_baseline and ws == 1:
         line["cpu_baseline"] = cpu_baseline(P_np, prob)
     return line
@@ -326,11 +426,13 @@ def run_reference(args, ws, rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--builds-per-step", type=int, default=STEP_BUILDS)
+    ap.add_argument("--no-solves", dest="solves", action="store_false",
+                    help="skip the whole-solve legs (SCF 24x24, CG 144x144, 64-solve density scan)")
     ap.add_argument("--no-extras", dest="extras", action="store_false",
                     help="skip the c64 / FP32-FFT variants and the e2e leg (short runs for profiling)")
     args = ap.parse_args()
