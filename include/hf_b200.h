@@ -259,6 +259,39 @@ int hf_cg_solve(void* stream, const hf_cg_problem* problem, const hf_cg_config* 
                 void* Q, void* p, void* density, void* fock, double* hist_E, double* hist_grad,
                 double* scalars_out, void* workspace, size_t workspace_bytes);
 
+/* ---- Reverse mode (complex128) -------------------------------------------------
+ * The reference differentiates build_fock / hf_energy / free_energy with
+ * jax.grad (fock.py:18-129 under jax autodiff); these are the hand-written
+ * adjoints behind the PyTorch autograd Functions of adjoint.py.  Gradients
+ * use torch's convention for complex leaves (d/dRe + i d/dIm).
+ *
+ * hf_fock_build_vjp: cotangents Sigma_bar, F_bar (either may be NULL) of the
+ * (Sigma, F) outputs of hf_fock_build -> P_bar = A^H(Sigma_bar + herm(F_bar))
+ * with A^H the exchange map run with VR_adj = conj(VR) (VR itself when real),
+ * and h_bar = herm(F_bar) (may be NULL).  Exchange part only: the Hartree and
+ * contact terms are linear maps of a few nb x nb reductions and are
+ * differentiated by the caller.  Workspace from hf_fock_vjp_workspace_size. */
+int hf_fock_vjp_workspace_size(int dtype, unsigned flags, int nk1, int nk2, int nb, size_t* bytes);
+int hf_fock_build_vjp(void* stream, int dtype, unsigned flags, int nk1, int nk2, int nb, const void* Sigma_bar,
+                      const void* F_bar, const void* VR_adj, void* P_bar, void* h_bar, void* workspace,
+                      size_t workspace_bytes);
+/* hf_energy_vjp: E = Re sum_k w_k tr((h + (Sigma + H)/2) P) with cotangent E_bar ->
+ * P_bar = E_bar w (h + (Sigma+H)/2)^H, h_bar = E_bar w P^H, Sigma_bar = E_bar w P^H / 2
+ * (each output may be NULL).  H_mode as hf_energy. */
+int hf_energy_vjp(void* stream, int nk1, int nk2, int nb, const void* P, const void* h, const void* Sigma,
+                  const void* H, int H_mode, const double* w2d, double E_bar, void* P_bar, void* h_bar,
+                  void* Sigma_bar);
+/* hf_free_energy_vjp: Omega = E - max(T,1e-14) S(p) -> p_bar = Omega_bar T w_norm (log p - log1p(-p))
+ * inside the entropy clip range [1e-14, 1-1e-14], 0 outside; E_bar = Omega_bar. */
+int hf_free_energy_vjp(void* stream, int nk1, int nk2, int nb, const double* p, const double* w_norm, double T,
+                       double Omega_bar, double* p_bar);
+/* hf_fourier_coeffs: out[r] = sum_k w_k exp(-i k.R_r) P_k for nR lattice vectors R (int pairs), k on
+ * the centred grid k_m = 2 pi (m - n/2) / n: the gradient of sum_k w_k Re tr(h_k P_k) with respect to
+ * an independent Fourier coefficient h_R of h_k = sum_R h_R exp(i k.R) (P Hermitian).  No counterpart
+ * in the reference (jax.grad through the user's Hamiltonian construction plays this role). */
+int hf_fourier_coeffs(void* stream, int nk1, int nk2, int nb, const void* P, const double* w2d, int nR,
+                      const int* R, void* out);
+
 /* Batched density scan: many independent CG solves, no host callbacks.  The
  * solves are ordered longest first (nk * nb^2 * (nb + 8)) and run n_lanes at a
  * time, each lane on its own stream (ordered after `stream`, which waits for all

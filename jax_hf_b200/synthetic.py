@@ -177,3 +177,32 @@ def density_scan(n: int = 64, seed: int = 4):
                                    V="scalar" if i % 2 == 0 else "layer", T=0.1,
                                    n_electrons=filling * nb, name=f"scan_{i}"))
     return out
+
+
+def coulomb_scalar_derivatives(nk: int, U: float = 1.0, d: float = 2.0):
+    """dV/dU and dV/dd of the gate-screened V(q) = U 2 pi tanh(|q| d) / |q| (V(0) = 0)."""
+    q = _qabs(nk)
+    dU = np.zeros_like(q)
+    dd = np.zeros_like(q)
+    nz = q > 0
+    dU[nz] = 2.0 * np.pi * np.tanh(q[nz] * d) / q[nz]
+    dd[nz] = U * 2.0 * np.pi / np.cosh(q[nz] * d) ** 2
+    return {"U": dU[..., None, None], "d": dd[..., None, None]}
+
+
+def coulomb_layer_derivatives(nk: int, nb: int, U: float = 1.0, d0: float = 1.0):
+    """dV/dU and dV/dd0 of the layer-resolved V_ab(q) with d_ab = d0 + |a - b| / 2."""
+    q = _qabs(nk)
+    nz = q > 0
+    dU = np.zeros((nk, nk, nb, nb))
+    dd = np.zeros((nk, nk, nb, nb))
+    for a in range(nb):
+        for b in range(nb):
+            dab = d0 + abs(a - b) / 2.0
+            t = np.zeros_like(q)
+            t[nz] = 2.0 * np.pi * np.tanh(q[nz] * dab) / q[nz]
+            dU[..., a, b] = t
+            s = np.zeros_like(q)
+            s[nz] = U * 2.0 * np.pi / np.cosh(q[nz] * dab) ** 2
+            dd[..., a, b] = s
+    return {"U": dU, "d": dd}

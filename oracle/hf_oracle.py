@@ -1064,3 +1064,28 @@ def solve_scf(kernel, P0, n_electrons, *, config=None, fock_build_fn=None):
     return dict(density_matrix=dens, fock_matrix=F_fin, energy=E_fin, chemical_potential=mu_fin,
                 iterations=k, converged=bool(converged),
                 history=dict(E=hE[:k], density_residual=hD[:k], commutator_residual=hC[:k]))
+
+
+# ------------------------------------------------------------ gradients ---
+# Partial derivatives of the objective at fixed density: what jax.grad of the
+# reference returns for build_fock + hf_energy (fock.py:18-111) with the density
+# held fixed; at a converged stationary point they are the total derivatives of
+# the converged free energy (envelope theorem).
+
+def coupling_gradient(kernel, P, dV):
+    """1/2 sum_k w_k Re tr(Sigma_{dV}[P - refP] P): d hf_energy / d theta for V -> V + theta dV."""
+    w = np.asarray(kernel.w2d, np.float64)
+    VR = _fftn(w[..., None, None] * np.asarray(dV, np.complex128)) * shift_phase(P.shape[0], P.shape[1])
+    dP = P - kernel.refP
+    Sd = _selfenergy_fft_full(VR, dP)
+    return float(0.5 * np.sum(w[..., None, None] * np.real(Sd * np.swapaxes(P, -1, -2))))
+
+
+def fourier_coefficient_gradient(P, w2d, R):
+    """sum_k w_k exp(-i k.R) P_k on the centred k grid: d E / d h_R for an independent h_R."""
+    nk1, nk2 = P.shape[0], P.shape[1]
+    k1 = 2.0 * np.pi * (np.arange(nk1) - nk1 // 2) / nk1
+    k2 = 2.0 * np.pi * (np.arange(nk2) - nk2 // 2) / nk2
+    K1, K2 = np.meshgrid(k1, k2, indexing="ij")
+    w = np.asarray(w2d, np.float64)
+    return np.stack([np.einsum("ij,ijab->ab", w * np.exp(-1j * (K1 * Rx + K2 * Ry)), P) for (Rx, Ry) in R])
