@@ -328,6 +328,48 @@ def run_solves(dev):
                       "all_converged": bool(all(bool(r.converged) for r in rb)),
                       "speedup_vs_fp64_solve_by_solve": round(sum(t_one) / ms, 3)}
     out["density_scan_64"] = scan
+    out["gradients_96x96_nb4"] = run_gradients(dev, ev_time)
+    return out
+
+
+def run_gradients(dev, ev_time):
+    """96x96 nb=4 scalar-V model: trust-region Newton (tol_grad 1e-6) and SCF-DIIS solves, then
+    d Omega*/d(U, d, h_R) through the hand-written adjoint at the converged density, with a
+    central difference of Omega in U at that density (step 1e-6) beside it."""
+    import torch
+    import jax_hf_b200 as G
+    from jax_hf_b200 import adjoint as A
+    from jax_hf_b200 import synthetic as S
+    from jax_hf_b200.reference_scf import SCFConfig, solve_scf
+    from jax_hf_b200.solver import SolverConfig, solve
+
+    p3 = S.newton_96()
+    K = G.HartreeFockKernel(**p3.kernel_kwargs())
+    P0 = torch.zeros((96, 96, 4, 4), dtype=torch.complex128, device=dev)
+    out = {}
+    ncfg = SolverConfig(optimizer="newton", tol_grad=1e-6, max_iter=200)
+    rn, ms_n = ev_time(lambda: solve(K, P0, p3.n_electrons, config=ncfg))
+    out["newton"] = {"ms_per_solve": round(ms_n, 2), "n_iter": int(rn.n_iter), "converged": bool(rn.converged),
+                     "energy": float(rn.energy)}
+    scfg = SCFConfig(acceleration="diis", density_tol=1e-10, comm_tol=1e-9, max_iter=300)
+    rs, ms_s = ev_time(lambda: solve_scf(K, P0, p3.n_electrons, config=scfg))
+    out["scf_diis"] = {"ms_per_solve": round(ms_s, 2), "iterations": int(rs.iterations),
+                       "converged": bool(rs.converged), "energy": float(rs.energy)}
+    dens = rs.density_matrix if bool(rs.converged) else rn.density
+    dV = S.coulomb_scalar_derivatives(96, 1.0, 2.0)
+    R = S.lattice_vectors(2.0)
+    A.parameter_gradients(K, dens, coupling_derivatives=dV, lattice_vectors=R)
+    g, ms_g = ev_time(lambda: A.parameter_gradients(K, dens, coupling_derivatives=dV, lattice_vectors=R), reps=3)
+    step = 1e-6
+
+    def e_at(U):
+        Kx = G.HartreeFockKernel(**dict(p3.kernel_kwargs(), coulomb_q=S.coulomb_scalar(96, U, 2.0)))
+        return float(A.objective(dens, torch.full((96, 96, 4), 0.5, dtype=torch.float64, device=dev), Kx))
+
+    fd_U = (e_at(1.0 + step) - e_at(1.0 - step)) / (2 * step)
+    out["gradients"] = {"ms": round(ms_g, 3), "n_params": 2 + len(R) * 16, "dOmega_dU": g["U"],
+                        "dOmega_dd": g["d"], "fd_dOmega_dU_fixed_density": fd_U,
+                        "rel_err_vs_fd": abs(fd_U - g["U"]) / max(abs(fd_U), 1e-300)}
     return out
 
 
