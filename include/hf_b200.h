@@ -48,7 +48,11 @@ extern "C" {
 #define HF_FOCK_FFT_FP32 (1u << 5)  /* complex128 storage, exchange FFT in FP32        */
 #define HF_FOCK_HAS_REFP (1u << 6)  /* refP is non-zero and must be subtracted         */
 #define HF_FOCK_GENERIC_FFT (1u << 7) /* force the generic shared-memory FFT engine    */
-
+/* V_ab(q) is real and V_ab = V_ba (caller asserts): with HF_FOCK_PACKING the
+ * Hermitian channel packing then also applies to a band-resolved V (only the
+ * upper-triangle channels are transformed, Sigma_ba = conj(Sigma_ab)); exact
+ * for a Hermitian density.  The reference packs scalar V only (utils.py:140-161). */
+#define HF_FOCK_SYM_V (1u << 8)
 const char* hf_last_error(void);
 const char* hf_status_string(int status);
 int hf_version(void);

@@ -29,6 +29,7 @@ FOCK_VR_REAL = 1 << 4
 FOCK_FFT_FP32 = 1 << 5
 FOCK_HAS_REFP = 1 << 6
 FOCK_GENERIC_FFT = 1 << 7
+FOCK_SYM_V = 1 << 8
 
 vp, i32, u32, f64, sz = C.c_void_p, C.c_int, C.c_uint, C.c_double, C.c_size_t
 pf64 = C.POINTER(C.c_double)

@@ -408,7 +408,7 @@ static int validate(int dtype, unsigned flags, int nk1, int nk2, int nb) {
   if (nb > kMaxNb) return fail(HF_ERR_UNSUPPORTED, "nb > 32 is not supported by this build");
   if (!(flags & (HF_FOCK_EXCHANGE | HF_FOCK_HARTREE)))
     return fail(HF_ERR_INVALID, "HartreeFockKernel must include at least one of Hartree or exchange.");
-  if ((flags & HF_FOCK_PACKING) && !(flags & HF_FOCK_VR_SCALAR))
+  if ((flags & HF_FOCK_PACKING) && !(flags & (HF_FOCK_VR_SCALAR | HF_FOCK_SYM_V)))
     return fail(HF_ERR_INVALID,
                 "hermitian_channel_packing requires a scalar interaction kernel with shape (..., 1, 1).");
   if ((flags & HF_FOCK_FFT_FP32) && dtype != HF_C128)

@@ -24,7 +24,7 @@ namespace cg = cooperative_groups;
 namespace hf {
 
 constexpr int kMuThreads = 1024;
-constexpr int kMuMaxCluster = 8;
+constexpr int kMuMaxCluster = 16;  // non-portable size, used when the device schedules it
 
 struct MuArgs {
   const void* eps;
@@ -43,6 +43,25 @@ __device__ __forceinline__ double load_eps(const MuArgs& a, int e) {
 template <typename RT>
 __device__ __forceinline__ double load_w(const MuArgs& a, int e) {
   return (double)static_cast<const RT*>(a.w)[e / a.nb];
+}
+
+// Visits the elements e = gt, gt + gs, ... < n in batches of U with all U loads of
+// a batch issued before any use, so each thread keeps U L2 requests in flight
+// instead of one (the passes are load-latency bound, not exp bound).
+template <typename RT, int U, class F>
+__device__ __forceinline__ void for_each_eps(const MuArgs& a, int gt, int gs, F&& f) {
+  for (int base = gt; base < a.n; base += U * gs) {
+    double ev[U], wv[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int e = base + u * gs;
+      ev[u] = e < a.n ? load_eps<RT>(a, e) : 0.0;
+      wv[u] = e < a.n ? load_w<RT>(a, e) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (base + u * gs < a.n) f(ev[u], wv[u]);
+  }
 }
 
 // cluster-wide sum of (x, y); every thread of every CTA receives the total.
@@ -109,11 +128,10 @@ __global__ void __launch_bounds__(kMuThreads) k_find_mu(const MuArgs a) {
   const int gs = cl.num_blocks() * blockDim.x;
 
   double mn = INFINITY, mx = -INFINITY;
-  for (int e = gt; e < a.n; e += gs) {
-    const double v = load_eps<RT>(a, e);
+  for_each_eps<RT, 4>(a, gt, gs, [&](double v, double) {
     mn = fmin(mn, v);
     mx = fmax(mx, v);
-  }
+  });
   cluster_minmax(cl, mn, mx, slots, wsm);
 
   int parity = 0;
@@ -126,8 +144,7 @@ __global__ void __launch_bounds__(kMuThreads) k_find_mu(const MuArgs a) {
     for (int it = 0; it < a.maxiter; ++it) {
       const double mid = 0.5 * (lo + hi);
       double cnt = 0.0, dummy = 0.0;
-      for (int e = gt; e < a.n; e += gs)
-        cnt += load_w<RT>(a, e) * expit(-(load_eps<RT>(a, e) - mid) / Td);
+      for_each_eps<RT, 4>(a, gt, gs, [&](double ev, double w) { cnt += w * expit(-(ev - mid) / Td); });
       cluster_sum2(cl, cnt, dummy, slots, wsm, parity);
       parity ^= 1;
       const double nlo = (cnt > a.target) ? lo : mid;
@@ -153,12 +170,11 @@ __global__ void __launch_bounds__(kMuThreads) k_find_mu(const MuArgs a) {
     }
     for (int it = 0; it < a.maxiter; ++it) {
       double N = 0.0, Z = 0.0;
-      for (int e = gt; e < a.n; e += gs) {
-        const double w = load_w<RT>(a, e);
-        const double p = expit((mu - load_eps<RT>(a, e)) / Tj);
+      for_each_eps<RT, 4>(a, gt, gs, [&](double ev, double w) {
+        const double p = expit((mu - ev) / Tj);
         N += w * p;
         Z += w * (p * (1.0 - p)) / Tj;
-      }
+      });
       cluster_sum2(cl, N, Z, slots, wsm, parity);
       parity ^= 1;
       const double g = N - a.target;
@@ -176,8 +192,7 @@ __global__ void __launch_bounds__(kMuThreads) k_find_mu(const MuArgs a) {
     }
     if (a.method == 1) {
       double N = 0.0, dummy = 0.0;
-      for (int e = gt; e < a.n; e += gs)
-        N += load_w<RT>(a, e) * expit((mu - load_eps<RT>(a, e)) / Tj);
+      for_each_eps<RT, 4>(a, gt, gs, [&](double ev, double w) { N += w * expit((mu - ev) / Tj); });
       cluster_sum2(cl, N, dummy, slots, wsm, parity);
       parity ^= 1;
       if (fabs(N - a.target) > 1e-12) mu = 0.5 * (lo + hi);
@@ -225,6 +240,32 @@ int hf::find_mu_internal(void* stream, int dtype, int method, int nk1, int nk2, 
   int csize = (a.n + 4 * kMuThreads - 1) / (4 * kMuThreads);
   if (csize < 1) csize = 1;
   if (csize > kMuMaxCluster) csize = kMuMaxCluster;
+  if (csize > 8) {  // beyond the portable 8: only as large as the device can co-schedule
+    const void* fn = single ? (const void*)k_find_mu<float> : (const void*)k_find_mu<double>;
+    static int max16[2][64] = {};  // per (precision, device): 0 unknown, else the largest schedulable size
+    int dev = 0;
+    HF_CUDA(cudaGetDevice(&dev));
+    int& mc = max16[single ? 1 : 0][dev & 63];
+    if (mc == 0) {
+      mc = 8;
+      if (cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
+        cudaLaunchConfig_t q = {};
+        q.gridDim = dim3(kMuMaxCluster, 1, 1);
+        q.blockDim = dim3(kMuThreads, 1, 1);
+        cudaLaunchAttribute qa[1];
+        qa[0].id = cudaLaunchAttributeClusterDimension;
+        qa[0].val.clusterDim.x = kMuMaxCluster;
+        qa[0].val.clusterDim.y = 1;
+        qa[0].val.clusterDim.z = 1;
+        q.attrs = qa;
+        q.numAttrs = 1;
+        int c = 0;
+        if (cudaOccupancyMaxPotentialClusterSize(&c, fn, &q) == cudaSuccess && c >= 8) mc = c < kMuMaxCluster ? c : kMuMaxCluster;
+      }
+      cudaGetLastError();  // a refused query leaves the portable size
+    }
+    if (csize > mc) csize = mc;
+  }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(csize, 1, 1);
   cfg.blockDim = dim3(kMuThreads, 1, 1);

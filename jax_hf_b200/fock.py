@@ -49,8 +49,15 @@ def build_fock(P, *, h, VR, refP, HH, w2d, include_exchange: bool, include_hartr
                exchange_hermitian_channel_packing: bool, contact_g=None, contact_Oi=None,
                contact_Oj=None, exchange_block_specs=None, exchange_check_offdiag=None,
                exchange_offdiag_atol: float = 1e-12, exchange_offdiag_rtol: float = 0.0,
-               project_fn=None, fft_precision=None, engine=None, out=None):
-    """Returns (Sigma, H, F) with F = herm(h + Sigma[P - refP] + H[P - refP]) (fock.py:18-97)."""
+               project_fn=None, fft_precision=None, engine=None, hermitian_density: bool = False, out=None):
+    """Returns (Sigma, H, F) with F = herm(h + Sigma[P - refP] + H[P - refP]) (fock.py:18-97).
+
+    Extensions (keyword-only, defaults keep the reference behaviour): ``fft_precision="fp32"``
+    runs the exchange FFT in FP32; ``engine="generic"`` forces the shared-memory FFT engine;
+    ``hermitian_density=True`` states that P (and refP) are Hermitian, which lets a kernel
+    whose V(q) is real and symmetric in the band pair use the Hermitian channel packing
+    (upper-triangle channels only) for a band-resolved V as well; ``out`` = (Sigma, H, F).
+    """
     h = _as_dev(h)
     dev = h.device
     _lib.require_cuda(h)
@@ -72,6 +79,7 @@ def build_fock(P, *, h, VR, refP, HH, w2d, include_exchange: bool, include_hartr
             project_fn=project_fn, fft_precision=fft_precision)
 
     flags = 0
+    sym_v = bool(getattr(VR, "_hf_v_pair_symmetric", False))
     if include_exchange:
         flags |= _lib.FOCK_EXCHANGE
     if include_hartree:
@@ -93,6 +101,8 @@ def build_fock(P, *, h, VR, refP, HH, w2d, include_exchange: bool, include_hartr
         if VRt is not None and tuple(VRt.shape[-2:]) != (1, 1):
             raise ValueError("hermitian_channel_packing requires a scalar interaction kernel with shape (..., 1, 1).")
         flags |= _lib.FOCK_PACKING
+    elif hermitian_density and include_exchange and sym_v and exchange_block_specs is None:
+        flags |= _lib.FOCK_PACKING | _lib.FOCK_SYM_V
     refPt = None
     if refP is not None and not is_marked_zero(refP):
         refPt = _as_dev(refP, dev, cdt)

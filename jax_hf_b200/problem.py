@@ -98,6 +98,13 @@ class HartreeFockKernel:
         else:
             VRdev = torch.as_tensor(np.ascontiguousarray(VRs64.astype(cdt)), device=dev)
         self._VR_shifted = VRdev
+        # V(q) real and V_ab = V_ba: Hermitian channel packing is exact for Hermitian densities
+        # with a band-resolved V too (used by the solvers and build_fock(hermitian_density=True))
+        Vr = np.asarray(Vq)
+        self.v_pair_symmetric = bool(not np.iscomplexobj(Vr) and (
+            Vr.shape[-2:] == (1, 1) or np.array_equal(Vr, np.swapaxes(Vr, -1, -2))))
+        if self.v_pair_symmetric:
+            VRdev._hf_v_pair_symmetric = True
         self.VR = torch.as_tensor(VR64.astype(cdt), device=dev)
 
         self.T = float(T)

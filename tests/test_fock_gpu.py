@@ -293,3 +293,52 @@ def test_fast_engine_matches_generic(cuda, n1, n2, nb, V):
     assert rel(Ff, Fg.cpu().numpy()) < TOL64
     Sm, _, Fm = G.build_fock(Pt, fft_precision="fp32", **kw)
     assert rel(Sm, Sg.cpu().numpy()) < TOL32
+
+
+SYM_CASES = [
+    (48, 48, 8, False, False, None),
+    (24, 36, 6, True, True, None),
+    (20, 14, 5, False, False, None),          # generic engine lengths
+    (48, 48, 8, False, False, "fp32"),
+    (48, 48, 8, False, False, "c64"),
+    (36, 36, 4, False, False, "generic"),
+]
+
+
+@pytest.mark.parametrize("nk1,nk2,nb,hartree,contact,mode", SYM_CASES)
+def test_fock_hermitian_density_packing_band_resolved(cuda, nk1, nk2, nb, hartree, contact, mode):
+    """hermitian_density=True with a real, pair-symmetric band-resolved V transforms only the
+    upper-triangle channels; for a Hermitian density the result equals the full reference build."""
+    prob, P, rng = _problem(nk1, nk2, nb, "layer", 17 + nk1 + nb)
+    kw = {}
+    if hartree:
+        ref = S.haar_density(max(nk1, nk2), nb, 98)[:nk1, :nk2] * 0.5
+        HH = rng.normal(size=(nb, nb))
+        kw.update(include_hartree=True, reference_density=np.ascontiguousarray(ref), hartree_matrix=HH + HH.T)
+    if contact:
+        Oa = rng.normal(size=(nb, nb)) + 1j * rng.normal(size=(nb, nb))
+        kw.update(contact_terms=[(0.3, Oa, Oa.conj().T)])
+    dtype = np.complex64 if mode == "c64" else np.complex128
+    K, Ko = _pair(prob, dtype=dtype, **kw)
+    assert K.v_pair_symmetric
+    extra = {"hermitian_density": True}
+    if mode == "fp32":
+        extra["fft_precision"] = "fp32"
+    if mode == "generic":
+        extra["engine"] = "generic"
+    (Sg, H, F), (So, Ho, Fo) = _fock_both(K, Ko, P.astype(dtype), **extra)
+    tol = TOL32 if mode in ("fp32", "c64") else TOL64
+    assert rel(Sg, So) < tol, "Sigma"
+    assert rel(F, Fo) < tol, "F"
+    Fn = F.cpu().numpy()
+    assert np.abs(Fn - np.conj(np.swapaxes(Fn, -1, -2))).max() == 0.0
+
+
+def test_fock_hermitian_density_packing_192(cuda):
+    """The benchmark workload (192x192, nb=8, layer V, Haar density) through the packed path."""
+    prob, P = S.fock_build_192()
+    K, Ko = _pair(prob)
+    (Sg, H, F), (So, Ho, Fo) = _fock_both(K, Ko, P, hermitian_density=True)
+    assert rel(Sg, So) < TOL64
+    assert rel(F, Fo) < TOL64
+
