@@ -1,15 +1,18 @@
-// Lane-per-row kernels of the device CG loop for nb <= 8.
+// Lane-per-column kernels of the device CG loop for nb <= 8.
 //
-// A group of G lanes (G = 4 for nb <= 4, else 8) owns one k-point and lane r of
-// the group holds row r of every nb x nb matrix in registers, so a warp works on
-// 32/G k-points at once.  Products read the other operand's rows from a per-group
-// shared-memory stage (the G lanes of a group read the same address: broadcast).
-// The retraction is the Cayley transform solved directly,
+// A group of G lanes (G = 4 for nb <= 4, else 8) owns one k-point and lane c of
+// the group holds column c of every nb x nb matrix in registers, so a warp works
+// on 32/G k-points at once and, for a fixed row, the lanes of a group touch
+// consecutive 16-byte elements: global loads and stores are coalesced without
+// staging.  A product A B takes B from the lane's own column and A from a
+// per-group shared-memory copy read by broadcast (row stride nb + 1, so a lane
+// reading along a row of the copy stays clear of bank conflicts).
+// The retraction solves the Cayley transform directly,
 //   U(tau) = (I + tau d / 2)^{-1} (I - tau d / 2) = 2 (I + tau d / 2)^{-1} - I,
 // the form of _cayley_retract (solver.py:122-138), by Gauss-Jordan elimination
 // with partial pivoting (|re| + |im| pivots, as LAPACK's izamax); it equals the
 // spectral form of the reference loop (solver.py:161-197, eigh(i d)) up to
-// rounding and costs ~5x fewer FP64 operations per trial than a Jacobi eigh.
+// rounding and needs ~5x fewer FP64 operations per trial than a Jacobi eigh.
 #pragma once
 
 #include "common.cuh"
@@ -21,7 +24,8 @@ template <int NB>
 struct RowGroup {
   static constexpr int G = NB <= 4 ? 4 : 8;  // lanes per k-point
   static constexpr int KPW = 32 / G;         // k-points per warp
-  static constexpr int LD = NB * NB + 1;     // stage stride (complex); +1 spreads the groups over banks
+  static constexpr int LP = NB + 1;          // row stride of a shared copy (complex)
+  static constexpr int MAT = NB * LP;        // one shared copy of an nb x nb matrix
 };
 constexpr int kRowWarps = 4;
 
@@ -53,99 +57,82 @@ __device__ __forceinline__ double2 crecip(double2 z) {
   return make_double2(z.x * s, -z.y * s);
 }
 
-// Row r of U(tau) into u[] and every row j of U into SU[j * NB + .] (natural order),
-// from row r of d (skew-Hermitian).  `on`: this lane holds a real row of a live
-// k-point.  SP: 2*NB complex per group for the pivot row.  Warp-uniform control flow.
-template <int NB, int G>
-__device__ __forceinline__ void cayley_rows(const double2 (&d)[NB], double tau, int r, bool on, double2* SP,
-                                            double2* SU, double2 (&u)[NB]) {
+// element r of a register column (r runtime): a select chain, no local memory
+template <int NB>
+__device__ __forceinline__ double2 pick(const double2 (&v)[NB], int r) {
+  double2 o = v[0];
+#pragma unroll
+  for (int i = 1; i < NB; ++i)
+    if (i == r) o = v[i];
+  return o;
+}
+
+// Column c of U(tau) into u[] from column c of d (skew-Hermitian).  `on`: this lane
+// holds a real column of a live k-point.  SC: NB complex (pivot column), SX: one
+// shared matrix copy.  Warp-uniform control flow.
+template <int NB>
+__device__ __forceinline__ void cayley_cols(const double2 (&d)[NB], double tau, int c, bool on, double2* SC,
+                                            double2* SX, double2 (&u)[NB]) {
+  constexpr int LP = RowGroup<NB>::LP;
   double2 m[NB], x[NB];
   const double h = 0.5 * tau;
 #pragma unroll
-  for (int c = 0; c < NB; ++c) {
-    m[c] = make_double2((c == r ? 1.0 : 0.0) + h * d[c].x, h * d[c].y);
-    x[c] = make_double2(c == r ? 1.0 : 0.0, 0.0);
+  for (int r = 0; r < NB; ++r) {
+    m[r] = make_double2((r == c ? 1.0 : 0.0) + h * d[r].x, h * d[r].y);
+    x[r] = make_double2(r == c ? 1.0 : 0.0, 0.0);
   }
-  bool used = false;
-  int mystep = 0;
+  unsigned used = 0;
+  int piv[NB];
 #pragma unroll
   for (int j = 0; j < NB; ++j) {
-    double key = (on && !used) ? fabs(m[j].x) + fabs(m[j].y) : -1.0;
-    int who = r;
+    if (on && c == j) {
 #pragma unroll
-    for (int off = G / 2; off > 0; off >>= 1) {
-      const double ok = __shfl_xor_sync(0xffffffffu, key, off);
-      const int ow = __shfl_xor_sync(0xffffffffu, who, off);
-      if (ok > key || (ok == key && ow < who)) {
-        key = ok;
-        who = ow;
-      }
-    }
-    if (r == who && on) {
-#pragma unroll
-      for (int c = 0; c < NB; ++c) {
-        SP[c] = m[c];
-        SP[NB + c] = x[c];
-      }
-      used = true;
-      mystep = j;
+      for (int r = 0; r < NB; ++r) SC[r] = m[r];
     }
     __syncwarp();
-    if (on && r != who) {
-      const double2 l = cmul(m[j], crecip(SP[j]));
+    // every lane finds the same pivot from the shared column (first maximum)
+    int p = 0;
+    double best = -1.0;
 #pragma unroll
-      for (int c = j; c < NB; ++c) m[c] = csub(m[c], cmul(l, SP[c]));
+    for (int r = 0; r < NB; ++r) {
+      const double2 v = SC[r];
+      const double key = ((used >> r) & 1u) ? -1.0 : fabs(v.x) + fabs(v.y);
+      if (key > best) { best = key; p = r; }
+    }
+    piv[j] = p;
+    used |= 1u << p;
+    if (on) {
+      const double2 ip = crecip(SC[p]);
+      const double2 mp = pick<NB>(m, p), xp = pick<NB>(x, p);
 #pragma unroll
-      for (int c = 0; c < NB; ++c) x[c] = csub(x[c], cmul(l, SP[NB + c]));
+      for (int r = 0; r < NB; ++r) {
+        if (r == p) continue;
+        const double2 l = cmul(SC[r], ip);
+        m[r] = csub(m[r], cmul(l, mp));
+        x[r] = csub(x[r], cmul(l, xp));
+      }
     }
     __syncwarp();
   }
-  // the lane that pivoted step s holds row s of the inverse times m[s]
+  // row piv[j] holds column j's only non-zero: (M^-1)[j][c] = x[piv[j]] / m_j, m_j = M'[piv[j]][j]
   if (on) {
-    double2 piv = m[0];
 #pragma unroll
-    for (int c = 1; c < NB; ++c)
-      if (c == mystep) piv = m[c];
-    const double2 ip = crecip(piv);
+    for (int r = 0; r < NB; ++r) SX[r * LP + c] = x[r];
+    int pc = piv[0];
 #pragma unroll
-    for (int c = 0; c < NB; ++c) {
-      const double2 v = cmul(x[c], ip);
-      SU[mystep * NB + c] = make_double2(2.0 * v.x - (c == mystep ? 1.0 : 0.0), 2.0 * v.y);
-    }
+    for (int i = 1; i < NB; ++i)
+      if (i == c) pc = piv[i];
+    SC[c] = pick<NB>(m, pc);  // lane c holds column c: its pivot entry M'[piv[c]][c]
   }
   __syncwarp();
   if (on) {
 #pragma unroll
-    for (int c = 0; c < NB; ++c) u[c] = SU[r * NB + c];
-  }
-}
-
-// eps_t[r] = Re (U^H Ft U)_rr from row r of Ft and the U rows in SU; SW: stage for W = Ft U.
-template <int NB>
-__device__ __forceinline__ double diag_uhfu_row(const double2 (&ft)[NB], int r, bool on, const double2* SU,
-                                                double2* SW) {
-  if (on) {
-    double2 w[NB];
-#pragma unroll
-    for (int n = 0; n < NB; ++n) w[n] = make_double2(0.0, 0.0);
-#pragma unroll
     for (int j = 0; j < NB; ++j) {
-#pragma unroll
-      for (int n = 0; n < NB; ++n) w[n] = cfma(ft[j], SU[j * NB + n], w[n]);
+      const double2 v = cmul(SX[piv[j] * LP + c], crecip(SC[j]));
+      u[j] = make_double2(2.0 * v.x - (j == c ? 1.0 : 0.0), 2.0 * v.y);
     }
-#pragma unroll
-    for (int n = 0; n < NB; ++n) SW[r * NB + n] = w[n];
   }
   __syncwarp();
-  double e = 0.0;
-  if (on) {
-#pragma unroll
-    for (int j = 0; j < NB; ++j) {
-      const double2 uj = SU[j * NB + r], wj = SW[j * NB + r];
-      e = fma(uj.x, wj.x, fma(uj.y, wj.y, e));
-    }
-  }
-  return e;
 }
 
 // ------------------------------------------------ density: p and P = herm(Q p Q^H)
@@ -153,49 +140,46 @@ template <int NB>
 __global__ void __launch_bounds__(32 * kRowWarps) k_cgr_density(CgArgs a, int force) {
   if (!force && !cg_active(a)) return;
   using RG = RowGroup<NB>;
-  constexpr int G = RG::G, KPW = RG::KPW, LD = RG::LD;
-  __shared__ double2 st[kRowWarps][KPW][2][LD];
+  constexpr int G = RG::G, KPW = RG::KPW, LP = RG::LP, MAT = RG::MAT;
+  __shared__ double2 st[kRowWarps][KPW][2 * MAT];
   __shared__ double spv[kRowWarps][KPW][NB];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, g = lane / G, r = lane % G;
-  double2* SQ = st[w][g][0];
-  double2* SX = st[w][g][1];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, g = lane / G, c = lane % G;
+  double2* SQ = st[w][g];
+  double2* SX = SQ + MAT;
   double* SPv = spv[w][g];
   const double mu = a.sc->mu, Tr = a.T_r;
   for (int kb = (blockIdx.x * kRowWarps + w) * KPW; kb < a.nk; kb += gridDim.x * kRowWarps * KPW) {
     const int k = kb + g;
-    const bool on = k < a.nk && r < NB;
-    const size_t row = ((size_t)k * NB + r) * NB;
-    double2 q[NB];
+    const bool on = k < a.nk && c < NB;
+    const size_t base = (size_t)k * NB * NB + c;
     if (on) {
 #pragma unroll
-      for (int m = 0; m < NB; ++m) {
-        q[m] = a.Q[row + m];
-        SQ[r * NB + m] = q[m];
-      }
-      const double pv = sigmoid((mu - a.eps[(size_t)k * NB + r]) / Tr);
-      a.p[(size_t)k * NB + r] = pv;
-      SPv[r] = pv;
+      for (int r = 0; r < NB; ++r) SQ[r * LP + c] = a.Q[base + (size_t)r * NB];
+      const double pv = sigmoid((mu - a.eps[(size_t)k * NB + c]) / Tr);
+      a.p[(size_t)k * NB + c] = pv;
+      SPv[c] = pv;
     }
     __syncwarp();
     double2 x[NB];
-    if (on) {
+    if (on) {  // X[r][c] = sum_n Q[r][n] p_n conj(Q[c][n])
+      double2 cq[NB];
 #pragma unroll
-      for (int n = 0; n < NB; ++n) q[n] = cscale(q[n], SPv[n]);
+      for (int n = 0; n < NB; ++n) cq[n] = cscale(conj(SQ[c * LP + n]), SPv[n]);
 #pragma unroll
-      for (int c = 0; c < NB; ++c) {
+      for (int r = 0; r < NB; ++r) {
         double2 acc = make_double2(0.0, 0.0);
 #pragma unroll
-        for (int n = 0; n < NB; ++n) acc = cfma_c(q[n], SQ[c * NB + n], acc);
-        x[c] = acc;
-        SX[r * NB + c] = acc;
+        for (int n = 0; n < NB; ++n) acc = cfma(SQ[r * LP + n], cq[n], acc);
+        x[r] = acc;
+        SX[r * LP + c] = acc;
       }
     }
     __syncwarp();
     if (on) {
 #pragma unroll
-      for (int c = 0; c < NB; ++c) {
-        const double2 y = SX[c * NB + r];
-        a.P[row + c] = make_double2(0.5 * (x[c].x + y.x), 0.5 * (x[c].y - y.y));
+      for (int r = 0; r < NB; ++r) {
+        const double2 y = SX[c * LP + r];  // X[c][r]
+        a.P[base + (size_t)r * NB] = make_double2(0.5 * (x[r].x + y.x), 0.5 * (x[r].y - y.y));
       }
     }
     __syncwarp();
@@ -207,90 +191,96 @@ template <int NB>
 __global__ void __launch_bounds__(32 * kRowWarps) k_cgr_grad1(CgArgs a) {
   if (!cg_active(a)) return;
   using RG = RowGroup<NB>;
-  constexpr int G = RG::G, KPW = RG::KPW, LD = RG::LD;
-  __shared__ double2 st[kRowWarps][KPW][2][LD];
+  constexpr int G = RG::G, KPW = RG::KPW, LP = RG::LP, MAT = RG::MAT;
+  __shared__ double2 st[kRowWarps][KPW][2 * MAT];
+  __shared__ double spv[kRowWarps][KPW][NB];
   __shared__ double red[64];
   __shared__ double tot[kMaxSums];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, g = lane / G, r = lane % G;
-  double2* SQ = st[w][g][0];
-  double2* ST = st[w][g][1];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, g = lane / G, c = lane % G;
+  double2* SQ = st[w][g];
+  double2* SF = SQ + MAT;  // F, then Ft
+  double* SPv = spv[w][g];
   const int par = a.sc->k & 1;
   double2* Gc = par ? a.G1 : a.G0;
   const double2* Gp = par ? a.G0 : a.G1;
   double* gp = par ? a.gp1 : a.gp0;
   const double* gpp = par ? a.gp0 : a.gp1;
   const double mu = a.sc->mu;
-  KSum acc[4];
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
   for (int kb = (blockIdx.x * kRowWarps + w) * KPW; kb < a.nk; kb += gridDim.x * kRowWarps * KPW) {
     const int k = kb + g;
-    const bool on = k < a.nk && r < NB;
-    const size_t row = ((size_t)k * NB + r) * NB;
-    double2 f[NB];
+    const bool on = k < a.nk && c < NB;
+    const size_t base = (size_t)k * NB * NB + c;
+    double2 q[NB];
     if (on) {
 #pragma unroll
-      for (int m = 0; m < NB; ++m) {
-        SQ[r * NB + m] = a.Q[row + m];
-        f[m] = a.F[row + m];
+      for (int r = 0; r < NB; ++r) {
+        q[r] = a.Q[base + (size_t)r * NB];
+        SQ[r * LP + c] = q[r];
+        SF[r * LP + c] = a.F[base + (size_t)r * NB];
       }
-    }
-    __syncwarp();
-    if (on) {  // T = F Q, row r
-#pragma unroll
-      for (int n = 0; n < NB; ++n) {
-        double2 t = make_double2(0.0, 0.0);
-#pragma unroll
-        for (int j = 0; j < NB; ++j) t = cfma(f[j], SQ[j * NB + n], t);
-        ST[r * NB + n] = t;
-      }
+      SPv[c] = a.p[(size_t)k * NB + c];
     }
     __syncwarp();
     double2 ft[NB];
-    if (on) {  // Ft = Q^H T, row r
+    if (on) {
+      double2 t[NB];  // T = F Q, column c
 #pragma unroll
-      for (int n = 0; n < NB; ++n) ft[n] = make_double2(0.0, 0.0);
+      for (int r = 0; r < NB; ++r) {
+        double2 acc = make_double2(0.0, 0.0);
 #pragma unroll
-      for (int i = 0; i < NB; ++i) {
-        const double2 qi = SQ[i * NB + r];
+        for (int j = 0; j < NB; ++j) acc = cfma(SF[r * LP + j], q[j], acc);
+        t[r] = acc;
+      }
 #pragma unroll
-        for (int n = 0; n < NB; ++n) ft[n] = cfma_cj(qi, ST[i * NB + n], ft[n]);
+      for (int m = 0; m < NB; ++m) {  // Ft = Q^H T, column c
+        double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int i = 0; i < NB; ++i) acc = cfma_cj(SQ[i * LP + m], t[i], acc);
+        ft[m] = acc;
       }
     }
     __syncwarp();
     if (on) {
 #pragma unroll
-      for (int n = 0; n < NB; ++n) {
-        SQ[r * NB + n] = ft[n];
-        a.Ft[row + n] = ft[n];
+      for (int m = 0; m < NB; ++m) {
+        SF[m * LP + c] = ft[m];
+        a.Ft[base + (size_t)m * NB] = ft[m];
       }
     }
     __syncwarp();
     if (on) {
       const double wk = a.w_norm[k];
-      const size_t vb = (size_t)k * NB;
-      const double pr = a.p[vb + r];
-      double ei = ft[0].x;
+      const double pc = SPv[c];
+      double ec = ft[0].x;
 #pragma unroll
-      for (int n = 0; n < NB; ++n) {
-        if (n == r) ei = ft[n].x;
+      for (int m = 0; m < NB; ++m) {  // element (i = m, j = c): 0.5 (p_j - p_i)(Ft_ij + conj(Ft_ji))
+        if (m == c) ec = ft[m].x;
         double2 gv = make_double2(0.0, 0.0);
-        if (n != r) {
-          const double2 fji = SQ[n * NB + r];
-          const double dpij = a.p[vb + n] - pr;
-          gv = make_double2(0.5 * dpij * (ft[n].x + fji.x), 0.5 * dpij * (ft[n].y - fji.y));
+        if (m != c) {
+          const double2 fji = SF[c * LP + m];
+          const double dpij = pc - SPv[m];
+          gv = make_double2(0.5 * dpij * (ft[m].x + fji.x), 0.5 * dpij * (ft[m].y - fji.y));
         }
-        Gc[row + n] = gv;
-        acc[0].add(wk * (gv.x * gv.x + gv.y * gv.y));
-        const double2 o = Gp[row + n];
-        acc[2].add(wk * (o.x * o.x + o.y * o.y));
+        Gc[base + (size_t)m * NB] = gv;
+        s0 += wk * (gv.x * gv.x + gv.y * gv.y);
+        const double2 o = Gp[base + (size_t)m * NB];
+        s2 += wk * (o.x * o.x + o.y * o.y);
       }
-      a.epsF[vb + r] = ei;
-      const double ps = clip(pr, 1e-6, 1.0 - 1e-6);
-      gp[vb + r] = ei + a.T_r * (log(ps) - log1p(-ps)) - mu;
-      acc[1].add(ei * ei);
-      acc[3].add(wk * gpp[vb + r] * gpp[vb + r]);
+      const size_t vb = (size_t)k * NB + c;
+      a.epsF[vb] = ec;
+      const double ps = clip(pc, 1e-6, 1.0 - 1e-6);
+      gp[vb] = ec + a.T_r * (log(ps) - log1p(-ps)) - mu;
+      s1 += ec * ec;
+      s3 += wk * gpp[vb] * gpp[vb];
     }
     __syncwarp();
   }
+  KSum acc[4];
+  acc[0].add(s0);
+  acc[1].add(s1);
+  acc[2].add(s2);
+  acc[3].add(s3);
   if (publish_partials<4>(acc, a.part, a.counter, red)) {
     gather_partials<4>(a.part, a.counter, tot, red);
     if (threadIdx.x == 0) {
@@ -303,21 +293,35 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_cgr_grad1(CgArgs a) {
   }
 }
 
+// eps_t[c] = Re (U^H Ft U)_cc from column c of U and the shared copy of Ft
+template <int NB>
+__device__ __forceinline__ double diag_uhfu_col(const double2 (&u)[NB], const double2* SFt) {
+  constexpr int LP = RowGroup<NB>::LP;
+  double e = 0.0;
+#pragma unroll
+  for (int j = 0; j < NB; ++j) {
+    double2 wj = make_double2(0.0, 0.0);  // W[j][c] = sum_l Ft[j][l] U[l][c]
+#pragma unroll
+    for (int l = 0; l < NB; ++l) wj = cfma(SFt[j * LP + l], u[l], wj);
+    e = fma(u[j].x, wj.x, fma(u[j].y, wj.y, e));
+  }
+  return e;
+}
+
 // -------------------- line-search trials i0 <= i < i1 on the frozen-F free energy
 template <int NB, int NT>
 __global__ void __launch_bounds__(32 * kRowWarps) k_cgr_trials(CgArgs a, int i0, int i1, int last_chunk) {
   if (!cg_active(a)) return;
   if (a.sc->accepted) return;
   using RG = RowGroup<NB>;
-  constexpr int G = RG::G, KPW = RG::KPW, LD = RG::LD;
-  __shared__ double2 st[kRowWarps][KPW][2][LD];
-  __shared__ double2 spiv[kRowWarps][KPW][2 * NB];
+  constexpr int G = RG::G, KPW = RG::KPW, LP = RG::LP, MAT = RG::MAT;
+  __shared__ double2 st[kRowWarps][KPW][2 * MAT + NB];
   __shared__ double red[64];
   __shared__ double tot[kMaxSums];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, g = lane / G, r = lane % G;
-  double2* SU = st[w][g][0];
-  double2* SW = st[w][g][1];
-  double2* SP = spiv[w][g];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, g = lane / G, c = lane % G;
+  double2* SFt = st[w][g];
+  double2* SX = SFt + MAT;
+  double2* SC = SX + MAT;
   const int nt = i1 - i0;
   double taus[NT];
   {
@@ -328,40 +332,49 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_cgr_trials(CgArgs a, int i0,
       tau = tau * a.bt_shrink;
     }
   }
-  KSum acc[2 * NT];
+  double se[NT], sh[NT];
+#pragma unroll
+  for (int i = 0; i < NT; ++i) se[i] = sh[i] = 0.0;
   for (int kb = (blockIdx.x * kRowWarps + w) * KPW; kb < a.nk; kb += gridDim.x * kRowWarps * KPW) {
     const int k = kb + g;
-    const bool on = k < a.nk && r < NB;
-    const size_t row = ((size_t)k * NB + r) * NB;
-    double2 d[NB], ft[NB];
+    const bool on = k < a.nk && c < NB;
+    const size_t base = (size_t)k * NB * NB + c;
+    double2 d[NB];
     double pv = 0.0, dpv = 0.0, wk = 0.0;
     if (on) {
 #pragma unroll
-      for (int m = 0; m < NB; ++m) {
-        d[m] = a.dQ[row + m];
-        ft[m] = a.Ft[row + m];
+      for (int r = 0; r < NB; ++r) {
+        d[r] = a.dQ[base + (size_t)r * NB];
+        SFt[r * LP + c] = a.Ft[base + (size_t)r * NB];
       }
-      pv = a.p[(size_t)k * NB + r];
-      dpv = a.dp[(size_t)k * NB + r];
+      pv = a.p[(size_t)k * NB + c];
+      dpv = a.dp[(size_t)k * NB + c];
       wk = a.w_norm[k];
     } else {
 #pragma unroll
-      for (int m = 0; m < NB; ++m) d[m] = ft[m] = make_double2(0.0, 0.0);
+      for (int r = 0; r < NB; ++r) d[r] = make_double2(0.0, 0.0);
     }
+    __syncwarp();
 #pragma unroll
     for (int it = 0; it < NT; ++it) {
       if (it < nt) {  // warp-uniform
         double2 u[NB];
-        cayley_rows<NB, G>(d, taus[it], r, on, SP, SU, u);
-        const double et = diag_uhfu_row<NB>(ft, r, on, SU, SW);
+        cayley_cols<NB>(d, taus[it], c, on, SC, SX, u);
         if (on) {
+          const double et = diag_uhfu_col<NB>(u, SFt);
           const double pt = clip(pv - taus[it] * dpv, 1e-8, 1.0 - 1e-8);
-          acc[2 * it].add(wk * pt * et);
-          acc[2 * it + 1].add(wk * ent_term(pt));
+          se[it] += wk * pt * et;
+          sh[it] += wk * ent_term(pt);
         }
-        __syncwarp();
       }
     }
+    __syncwarp();
+  }
+  KSum acc[2 * NT];
+#pragma unroll
+  for (int i = 0; i < NT; ++i) {
+    acc[2 * i].add(se[i]);
+    acc[2 * i + 1].add(sh[i]);
   }
   if (publish_partials<2 * NT>(acc, a.part, a.counter, red)) {
     gather_partials<2 * NT>(a.part, a.counter, tot, red);
@@ -386,43 +399,44 @@ template <int NB>
 __global__ void __launch_bounds__(32 * kRowWarps) k_cgr_update(CgArgs a) {
   if (!cg_active(a)) return;
   using RG = RowGroup<NB>;
-  constexpr int G = RG::G, KPW = RG::KPW, LD = RG::LD;
-  __shared__ double2 st[kRowWarps][KPW][2][LD];
-  __shared__ double2 spiv[kRowWarps][KPW][2 * NB];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, g = lane / G, r = lane % G;
-  double2* SU = st[w][g][0];
-  double2* SW = st[w][g][1];
-  double2* SP = spiv[w][g];
+  constexpr int G = RG::G, KPW = RG::KPW, LP = RG::LP, MAT = RG::MAT;
+  __shared__ double2 st[kRowWarps][KPW][2 * MAT + NB];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, g = lane / G, c = lane % G;
+  double2* SFt = st[w][g];
+  double2* SX = SFt + MAT;  // Cayley stage, then the copy of Q
+  double2* SC = SX + MAT;
   const double tau = a.sc->tau_final;
   for (int kb = (blockIdx.x * kRowWarps + w) * KPW; kb < a.nk; kb += gridDim.x * kRowWarps * KPW) {
     const int k = kb + g;
-    const bool on = k < a.nk && r < NB;
-    const size_t row = ((size_t)k * NB + r) * NB;
-    double2 d[NB], ft[NB];
+    const bool on = k < a.nk && c < NB;
+    const size_t base = (size_t)k * NB * NB + c;
+    double2 d[NB];
     if (on) {
 #pragma unroll
-      for (int m = 0; m < NB; ++m) {
-        d[m] = a.dQ[row + m];
-        ft[m] = a.Ft[row + m];
+      for (int r = 0; r < NB; ++r) {
+        d[r] = a.dQ[base + (size_t)r * NB];
+        SFt[r * LP + c] = a.Ft[base + (size_t)r * NB];
       }
     } else {
 #pragma unroll
-      for (int m = 0; m < NB; ++m) d[m] = ft[m] = make_double2(0.0, 0.0);
+      for (int r = 0; r < NB; ++r) d[r] = make_double2(0.0, 0.0);
     }
+    __syncwarp();
     double2 u[NB];
-    cayley_rows<NB, G>(d, tau, r, on, SP, SU, u);
-    const double et = diag_uhfu_row<NB>(ft, r, on, SU, SW);
+    cayley_cols<NB>(d, tau, c, on, SC, SX, u);  // ends with a warp barrier: SX is free again
     if (on) {
-      a.eps[(size_t)k * NB + r] = et;
-      double2 q[NB];
+      a.eps[(size_t)k * NB + c] = diag_uhfu_col<NB>(u, SFt);
 #pragma unroll
-      for (int m = 0; m < NB; ++m) q[m] = a.Q[row + m];
+      for (int r = 0; r < NB; ++r) SX[r * LP + c] = a.Q[base + (size_t)r * NB];
+    }
+    __syncwarp();
+    if (on) {
 #pragma unroll
-      for (int n = 0; n < NB; ++n) {
+      for (int r = 0; r < NB; ++r) {  // (Q U)[r][c] = sum_j Q[r][j] U[j][c]
         double2 acc = make_double2(0.0, 0.0);
 #pragma unroll
-        for (int j = 0; j < NB; ++j) acc = cfma(q[j], SU[j * NB + n], acc);
-        a.Q[row + n] = acc;
+        for (int j = 0; j < NB; ++j) acc = cfma(SX[r * LP + j], u[j], acc);
+        a.Q[base + (size_t)r * NB] = acc;
       }
     }
     __syncwarp();

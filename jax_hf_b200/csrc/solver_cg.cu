@@ -95,6 +95,10 @@ __global__ void k_cg_init(CgArgs a, const double2* __restrict__ P0, const double
   }
 }
 
+// Rotation threshold of the init / finalize eigensolves, relative to |A|_F: at the
+// double-precision rounding level, so converged rotations are not re-made from noise.
+constexpr double kEigTol = 1e-15;
+
 // eps, Q <- eigh(A) per k (A = F0 at init, or Ft = Q^H F Q at finalize with Q <- Q V)
 __global__ void k_cg_eig(CgArgs a, const double2* __restrict__ A, int rotate) {
   extern __shared__ double2 sm[];
@@ -130,7 +134,7 @@ __global__ void k_cg_eig(CgArgs a, const double2* __restrict__ A, int rotate) {
       }
     }
     __syncwarp();
-    warp_jacobi_eigh(m, v, scr + nb, nb, lane, 1e-17);
+    warp_jacobi_eigh(m, v, scr + nb, nb, lane, kEigTol);
     for (int e = lane; e < nb; e += 32) wv[e] = m[e * nb + e].x;
     __syncwarp();
     for (int i = lane; i < nb; i += 32) {
@@ -252,6 +256,104 @@ __device__ __forceinline__ double2 precond(double2 g, double ei, double ej, doub
   const double gap = ei - ej;
   const double d = sqrt(gap * gap + lam * lam);
   return make_double2(g.x / d, g.y / d);
+}
+
+// Elementwise passes with the band count as a template parameter (index math at
+// compile time), one rsqrt per element for the preconditioner, per-thread plain
+// double partials and compensated sums across threads and blocks.
+template <int NB>
+__global__ void __launch_bounds__(256) k_cg_grad2_t(CgArgs a) {
+  if (!cg_active(a)) return;
+  __shared__ double red[64];
+  __shared__ double tot[kMaxSums];
+  constexpr unsigned nb2 = NB * NB;
+  const int par = a.sc->k & 1;
+  const double2* G = par ? a.G1 : a.G0;
+  const double2* Gp = par ? a.G0 : a.G1;
+  const double* gp = par ? a.gp1 : a.gp0;
+  const double* gpp = par ? a.gp0 : a.gp1;
+  const double lam2 = a.sc->lam * a.sc->lam;
+  const unsigned nq = (unsigned)a.nk * nb2;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < nq; e += gridDim.x * blockDim.x) {
+    const unsigned k = e / nb2, r = e - k * nb2, i = r / NB, j = r - i * NB;
+    const double wk = a.w_norm[k];
+    const double2 g = G[e], o = Gp[e];
+    const double gap = a.epsF[k * NB + i] - a.epsF[k * NB + j];
+    const double rs = rsqrt(fma(gap, gap, lam2));
+    s0 += wk * rs * (g.x * g.x + g.y * g.y);
+    s1 += wk * rs * (o.x * g.x + o.y * g.y);
+    if (j == 0) {
+      const unsigned vi = k * NB + i;
+      const double ps = clip(a.p[vi], 1e-8, 1.0 - 1e-8);
+      const double hp = gp[vi] * (ps * (1.0 - ps) / a.T_r);
+      s2 += wk * gp[vi] * hp;
+      s3 += wk * gpp[vi] * hp;
+    }
+  }
+  KSum acc[4];
+  acc[0].add(s0);
+  acc[1].add(s1);
+  acc[2].add(s2);
+  acc[3].add(s3);
+  if (publish_partials<4>(acc, a.part, a.counter, red)) {
+    gather_partials<4>(a.part, a.counter, tot, red);
+    if (threadIdx.x == 0) {
+      CgScalars* sc = a.sc;
+      const double num = tot[0] - tot[1] + tot[2] - tot[3];
+      double beta = sc->pr_den > 1e-30 ? fmax(0.0, num / sc->pr_den) : 0.0;
+      beta = fmin(beta, 5.0);
+      if (sc->k == 0 || sc->k % a.cg_restart == 0) beta = 0.0;
+      sc->beta = beta;
+    }
+  }
+}
+
+template <int NB>
+__global__ void __launch_bounds__(256) k_cg_dir_t(CgArgs a) {
+  if (!cg_active(a)) return;
+  __shared__ double red[64];
+  __shared__ double tot[kMaxSums];
+  constexpr unsigned nb2 = NB * NB;
+  const int par = a.sc->k & 1;
+  const double2* G = par ? a.G1 : a.G0;
+  const double* gp = par ? a.gp1 : a.gp0;
+  const double lam2 = a.sc->lam * a.sc->lam, beta = a.sc->beta;
+  const unsigned nq = (unsigned)a.nk * nb2, nv = (unsigned)a.nk * NB;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < nq; e += gridDim.x * blockDim.x) {
+    const unsigned k = e / nb2, r = e - k * nb2, i = r / NB, j = r - i * NB;
+    const double gap = a.epsF[k * NB + i] - a.epsF[k * NB + j];
+    const double rs = rsqrt(fma(gap, gap, lam2));
+    const double2 g = G[e], dprev = a.dQ[e];
+    const double2 d = make_double2(fma(g.x, rs, beta * dprev.x), fma(g.y, rs, beta * dprev.y));
+    a.dQ[e] = d;
+    s0 += a.w_norm[k] * (d.x * d.x + d.y * d.y);
+  }
+  for (unsigned v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
+    const unsigned k = v / NB;
+    const double wk = a.w_norm[k];
+    const double ps = clip(a.p[v], 1e-8, 1.0 - 1e-8);
+    const double hp = gp[v] * (ps * (1.0 - ps) / a.T_r);
+    a.dp[v] = hp + beta * a.dp[v];
+    s1 += wk * ps * a.epsF[v];
+    s2 += wk * ent_term(ps);
+  }
+  KSum acc[3];
+  acc[0].add(s0);
+  acc[1].add(s1);
+  acc[2].add(s2);
+  if (publish_partials<3>(acc, a.part, a.counter, red)) {
+    gather_partials<3>(a.part, a.counter, tot, red);
+    if (threadIdx.x == 0) {
+      CgScalars* sc = a.sc;
+      const double dn = sqrt(fmax(0.0, tot[0]));
+      sc->tau0 = fmin(1.0, a.max_step / fmax(dn, 1e-30));
+      sc->Omega0 = tot[1] + fmax(a.T_r, 1e-14) * tot[2];
+      sc->accepted = 0;
+      sc->tau_final = sc->tau0;
+    }
+  }
 }
 
 // --------------------------------------------- grad2: PR+ inner products ---
@@ -639,6 +741,13 @@ static int cg_mu(CgRun& r, cudaStream_t s, int maxiter, const int* active) {
                           maxiter, &r.a.sc->mu, &r.a.sc->mu, active);
 }
 
+// Grid of an elementwise pass: a few elements per thread, at most 8 CTAs of 256 per SM.
+static int elem_blocks(size_t n) {
+  size_t b = (n + 4 * 256 - 1) / (4 * 256);
+  if (b > (size_t)148 * 8) b = 148 * 8;
+  return b < 1 ? 1 : (int)b;
+}
+
 // One iteration on the lane-per-row kernels (nb <= 8).
 template <int NB>
 static int cg_iteration_rows(CgRun& r, cudaStream_t s, const hf_cg_config& cf, bool fp32) {
@@ -653,10 +762,11 @@ static int cg_iteration_rows(CgRun& r, cudaStream_t s, const hf_cg_config& cf, b
   if ((st = cg_energy(r, s, &r.a.sc->E, act))) return st;
   k_cgr_grad1<NB><<<rb, 32 * kRowWarps, 0, s>>>(r.a);
   HF_LAUNCH_CHECK("k_cgr_grad1");
-  k_cg_grad2<<<eb, 256, 0, s>>>(r.a);
+  const int gb = elem_blocks((size_t)r.a.nk * NB * NB);
+  k_cg_grad2_t<NB><<<gb, 256, 0, s>>>(r.a);
   HF_LAUNCH_CHECK("k_cg_grad2");
-  k_cg_dir_lu<<<eb, 256, 0, s>>>(r.a);
-  HF_LAUNCH_CHECK("k_cg_dir_lu");
+  k_cg_dir_t<NB><<<gb, 256, 0, s>>>(r.a);
+  HF_LAUNCH_CHECK("k_cg_dir");
   const int bt = cf.bt_max;
   if (bt >= 1) {
     k_cgr_trials<NB, 1><<<rb, 32 * kRowWarps, 0, s>>>(r.a, 0, 1, bt == 1);
@@ -692,6 +802,14 @@ static int cg_density(CgRun& r, cudaStream_t s, int force) {
   const int nb = r.a.nb, nb2 = nb * nb;
   k_cg_density<<<r.nblk, 32 * kSolverWarps, (2 * (size_t)nb2 + nb) * 16 * kSolverWarps, s>>>(r.a, force);
   HF_LAUNCH_CHECK("k_cg_density");
+  return HF_OK;
+}
+
+// eps, Q <- eigh(A) (init) or eigh(Q^H F Q) with Q <- Q V (finalize)
+static int cg_eig(CgRun& r, cudaStream_t s, const double2* A, int rotate) {
+  const int nb = r.a.nb;
+  k_cg_eig<<<r.nblk, 32 * kSolverWarps, smem_eig(nb), s>>>(r.a, A, rotate);
+  HF_LAUNCH_CHECK("k_cg_eig");
   return HF_OK;
 }
 
@@ -893,8 +1011,7 @@ int CgSolver::start(const void* P0) {
                                    pb->weight_sum);
   HF_LAUNCH_CHECK("k_cg_init");
   if ((st = cg_fock(r, s, false, nullptr))) return st;
-  k_cg_eig<<<r.nblk, 32 * kSolverWarps, smem_eig(nb), s>>>(a, a.F, 0);
-  HF_LAUNCH_CHECK("k_cg_eig");
+  if ((st = cg_eig(r, s, a.F, 0))) return st;
   if ((st = cg_mu(r, s, cf->mu_maxiter, nullptr))) return st;
   return cf->max_iter > 0 ? launch_chunk() : launch_finalize();
 }
@@ -969,8 +1086,7 @@ int CgSolver::launch_finalize() {
   if ((st = cg_density(r, s, 1))) return st;
   if ((st = cg_project(r, s))) return st;
   if ((st = cg_fock(r, s, false, nullptr))) return st;
-  k_cg_eig<<<r.nblk, 32 * kSolverWarps, smem_eig(nb), s>>>(a, a.F, 1);
-  HF_LAUNCH_CHECK("k_cg_eig");
+  if ((st = cg_eig(r, s, a.F, 1))) return st;
   if ((st = cg_mu(r, s, cf->mu_maxiter, nullptr))) return st;
   if ((st = cg_density(r, s, 1))) return st;
   if ((st = cg_project(r, s))) return st;
