@@ -127,14 +127,33 @@ __global__ void __launch_bounds__(kMuThreads) k_find_mu(const MuArgs a) {
   const int gt = cl.block_rank() * blockDim.x + threadIdx.x;
   const int gs = cl.num_blocks() * blockDim.x;
 
-  double mn = INFINITY, mx = -INFINITY;
-  for_each_eps<RT, 4>(a, gt, gs, [&](double v, double) {
-    mn = fmin(mn, v);
-    mx = fmax(mx, v);
-  });
+  // Method 2 with a warm start: the min/max pass also forms N and Z at mu0, which
+  // are the first Newton evaluation whenever mu0 lies inside the bracket.
+  const bool fuse_first = a.method == 2 && a.mu0 != nullptr;
+  const double mu0v = fuse_first ? a.mu0[0] : 0.0;
+  const double Tf = fmax(a.T, 1e-12);
+  double mn = INFINITY, mx = -INFINITY, N0 = 0.0, Z0 = 0.0;
+  if (fuse_first) {
+    for_each_eps<RT, 4>(a, gt, gs, [&](double v, double w) {
+      mn = fmin(mn, v);
+      mx = fmax(mx, v);
+      const double p = expit((mu0v - v) / Tf);
+      N0 += w * p;
+      Z0 += w * (p * (1.0 - p)) / Tf;
+    });
+  } else {
+    for_each_eps<RT, 4>(a, gt, gs, [&](double v, double) {
+      mn = fmin(mn, v);
+      mx = fmax(mx, v);
+    });
+  }
   cluster_minmax(cl, mn, mx, slots, wsm);
-
   int parity = 0;
+  if (fuse_first) {
+    cluster_sum2(cl, N0, Z0, slots, wsm, parity);
+    parity ^= 1;
+  }
+
   double result;
   if (a.method == 0) {
     const double T = a.T;
@@ -168,15 +187,21 @@ __global__ void __launch_bounds__(kMuThreads) k_find_mu(const MuArgs a) {
       const double m0 = a.mu0 ? a.mu0[0] : 0.0;
       mu = fmin(fmax(m0, lo), hi);
     }
+    const bool have_first = fuse_first && mu == mu0v;
     for (int it = 0; it < a.maxiter; ++it) {
       double N = 0.0, Z = 0.0;
-      for_each_eps<RT, 4>(a, gt, gs, [&](double ev, double w) {
-        const double p = expit((mu - ev) / Tj);
-        N += w * p;
-        Z += w * (p * (1.0 - p)) / Tj;
-      });
-      cluster_sum2(cl, N, Z, slots, wsm, parity);
-      parity ^= 1;
+      if (it == 0 && have_first) {
+        N = N0;
+        Z = Z0;
+      } else {
+        for_each_eps<RT, 4>(a, gt, gs, [&](double ev, double w) {
+          const double p = expit((mu - ev) / Tj);
+          N += w * p;
+          Z += w * (p * (1.0 - p)) / Tj;
+        });
+        cluster_sum2(cl, N, Z, slots, wsm, parity);
+        parity ^= 1;
+      }
       const double g = N - a.target;
       if (g < 0) lo = mu;
       if (g > 0) hi = mu;
