@@ -329,6 +329,20 @@ def run_solves(dev):
                       "speedup_vs_fp64_solve_by_solve": round(sum(t_one) / ms, 3)}
     out["density_scan_64"] = scan
     out["gradients_96x96_nb4"] = run_gradients(dev, ev_time)
+    import torch.distributed as dist
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        # the 64 solves sharded over the ranks (greedy longest-first), FP64, batched per rank
+        from jax_hf_b200.scan import batched_runner, scan_shapes, solve_scan
+        run_local = batched_runner(probs, c64, lanes=16, device=dev)
+        dist.barrier()
+        res, ms = ev_time(lambda: solve_scan(scan_shapes(probs), run_local))
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        Es = np.array([r["energy"] for r in res])
+        scan["fp64_sharded_over_ranks"] = {
+            "ranks": dist.get_world_size(), "solves_per_s": round(len(probs) / (float(t) / 1e3), 2),
+            "total_ms_max_over_ranks": round(float(t), 2),
+            "max_rel_dE_vs_fp64": float((np.abs(Es - E_one) / np.abs(E_one)).max())}
     return out
 
 
