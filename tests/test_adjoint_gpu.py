@@ -175,3 +175,36 @@ def test_envelope_gradients_match_resolved_finite_differences(cuda):
     fd_im = (om_h(1j * step) - om_h(-1j * step)) / (2 * step)
     assert abs(fd_re - an_re) <= 1e-6 * max(abs(fd_re), 1e-3), (fd_re, an_re)
     assert abs(fd_im - an_im) <= 1e-6 * max(abs(fd_im), 1e-3), (fd_im, an_im)
+
+
+def test_torch_library_ops(cuda):
+    """torch.ops.hf_b200.fock_build / hf_energy: same values as the Python API, opcheck, gradients."""
+    import jax_hf_b200 as G
+    from jax_hf_b200 import torch_ops  # noqa: F401  (registers the ops)
+    nk, nb = 6, 3
+    K = G.HartreeFockKernel(**_kernel_kwargs(nk, nb, "layer", 51))
+    a = K.as_args()
+    P = torch.as_tensor(S.haar_density(nk, nb, 5), device="cuda")
+    h = K.h.to(torch.complex128).contiguous()
+    VR = a["VR"]
+    Sg, H, F = torch.ops.hf_b200.fock_build(P, h, VR, True, False)
+    S2, _, F2 = G.build_fock(P, h=h, VR=VR, refP=None, HH=None, w2d=None, include_exchange=True,
+                             include_hartree=False, exchange_hermitian_channel_packing=False)
+    assert torch.equal(Sg, S2) and torch.equal(F, F2)
+    w = K.w2d.to(torch.float64)
+    E = torch.ops.hf_b200.hf_energy(P, h, Sg, H, w)
+    assert abs(float(E) - float(G.hf_energy(P, h=h, Sigma=Sg, H=H, weights_b=w[..., None, None]))) == 0.0
+    torch.library.opcheck(torch.ops.hf_b200.fock_build.default, (P, h, VR, True, False),
+                          test_utils=("test_schema", "test_faketensor", "test_autograd_registration"))
+    torch.library.opcheck(torch.ops.hf_b200.hf_energy.default, (P, h, Sg, H, w),
+                          test_utils=("test_schema", "test_faketensor", "test_autograd_registration"))
+    # gradients through the ops against the autograd Functions of adjoint.py
+    from jax_hf_b200 import adjoint as A
+    P1, h1 = P.clone().requires_grad_(True), h.clone().requires_grad_(True)
+    Sg1, H1, _ = torch.ops.hf_b200.fock_build(P1, h1, VR, True, False)
+    torch.ops.hf_b200.hf_energy(P1, h1, Sg1, H1, w).backward()
+    P2, h2 = P.clone().requires_grad_(True), h.clone().requires_grad_(True)
+    Sg2, H2, _ = A.fock_build(P2, h2, K)
+    A.hf_energy(P2, h2, Sg2, H2, K.w2d).backward()
+    torch.testing.assert_close(P1.grad, P2.grad, rtol=0, atol=1e-13)
+    torch.testing.assert_close(h1.grad, h2.grad, rtol=0, atol=1e-13)
