@@ -443,4 +443,219 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_cgr_update(CgArgs a) {
   }
 }
 
+// ----------------------------------------------------------- eigensolver ---
+// Cyclic Jacobi for Hermitian A (Jacobi 1846; Golub & Van Loan 8.5, complex
+// rotations; round-robin pair order as the warp-per-matrix solver in perk.cuh)
+// in the lane-per-column layout with A and V kept in shared memory, lane c owning
+// column c.  Per round: the lane holding column q of each pair (p, q) computes the
+// rotation once; every lane forms its new columns of A G and V G in registers from
+// its own and its partner's column, writes them back, then applies the row mix
+// G^H A of every pair to its own column in place.  Rounds are a runtime loop, so
+// the code stays small.  Sweeps continue while any group of the warp rotated.
+template <int NB>
+struct JacobiPairs {
+  static constexpr int M = NB + (NB & 1);
+  __host__ __device__ static int pa(int t, int k) { return k == 0 ? 0 : 1 + ((k - 1 + t) % (M - 1)); }
+  __host__ __device__ static int pb(int t, int k) { return 1 + ((M - 1 - k - 1 + t) % (M - 1)); }
+};
+
+template <int NB>
+__device__ __forceinline__ void jacobi_smem_cols(double2* SA, double2* SV, double2* SP, int c, bool on,
+                                                 double thr) {
+  constexpr int LP = RowGroup<NB>::LP, M = JacobiPairs<NB>::M, NP = M / 2;
+  if (NB == 1) return;
+  for (int sweep = 0; sweep < 60; ++sweep) {
+    bool rotated = false;
+    for (int t = 0; t < M - 1; ++t) {
+      int partner = -1, kk = -1;
+      bool isq = false;
+#pragma unroll
+      for (int k = 0; k < NP; ++k) {
+        const int a0 = JacobiPairs<NB>::pa(t, k), b0 = JacobiPairs<NB>::pb(t, k);
+        const int p = a0 < b0 ? a0 : b0, q = a0 < b0 ? b0 : a0;
+        if (q < NB) {
+          if (c == p) { partner = q; kk = k; }
+          if (c == q) { partner = p; kk = k; isq = true; }
+        }
+      }
+      if (on && isq) {
+        const int p = partner;
+        const double2 apq = SA[p * LP + c];
+        const double mag = hypot(apq.x, apq.y);
+        double cc = 1.0, act = 0.0;
+        double2 sp = make_double2(0.0, 0.0);
+        if (mag > thr) {
+          const double app = SA[p * LP + p].x, aqq = SA[c * LP + c].x;
+          const double tau = (aqq - app) / (2.0 * mag);
+          const double tt = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+          cc = 1.0 / sqrt(1.0 + tt * tt);
+          const double sn = tt * cc;
+          sp = make_double2(sn * apq.x / mag, sn * apq.y / mag);
+          act = 1.0;
+        }
+        SP[2 * kk] = make_double2(cc, act);
+        SP[2 * kk + 1] = sp;
+      }
+      __syncwarp();
+      // A <- A G, V <- V G on this lane's column: new = cc own + beta partner
+      double cc = 1.0, act = 0.0;
+      double2 sp = make_double2(0.0, 0.0);
+      if (kk >= 0) {
+        const double2 h = SP[2 * kk];
+        cc = h.x;
+        act = h.y;
+        sp = SP[2 * kk + 1];
+      }
+      rotated = rotated || (on && act != 0.0);
+      const double2 beta = isq ? sp : make_double2(-sp.x, sp.y);  // q: sp;  p: -conj(sp)
+      double2 na[NB], nv[NB];
+      const bool mix = on && act != 0.0;
+      if (mix) {
+#pragma unroll
+        for (int r = 0; r < NB; ++r) {
+          na[r] = cadd(cscale(SA[r * LP + c], cc), cmul(beta, SA[r * LP + partner]));
+          nv[r] = cadd(cscale(SV[r * LP + c], cc), cmul(beta, SV[r * LP + partner]));
+        }
+      }
+      __syncwarp();
+      if (mix) {
+#pragma unroll
+        for (int r = 0; r < NB; ++r) {
+          SA[r * LP + c] = na[r];
+          SV[r * LP + c] = nv[r];
+        }
+      }
+      // A <- G^H A: rows p and q of this lane's column, every active pair; then exact zeros
+      if (on) {
+#pragma unroll
+        for (int k = 0; k < NP; ++k) {
+          const int a0 = JacobiPairs<NB>::pa(t, k), b0 = JacobiPairs<NB>::pb(t, k);
+          const int p = a0 < b0 ? a0 : b0, q = a0 < b0 ? b0 : a0;
+          if (q >= NB) continue;
+          const double2 hk = SP[2 * k];
+          if (hk.y == 0.0) continue;
+          const double2 spk = SP[2 * k + 1];
+          const double2 x = SA[p * LP + c], y = SA[q * LP + c];
+          SA[p * LP + c] = csub(cscale(x, hk.x), cmul(spk, y));
+          SA[q * LP + c] = cadd(cmulc(x, spk), cscale(y, hk.x));
+        }
+        if (act != 0.0) {
+          SA[partner * LP + c] = make_double2(0.0, 0.0);
+          SA[c * LP + c].y = 0.0;
+        }
+      }
+      __syncwarp();
+    }
+    if (!__any_sync(0xffffffffu, rotated)) break;
+  }
+}
+
+// eps, Q <- eigh(A) per k (A = F0 at init; Ft = Q^H F Q at finalize, then Q <- Q V),
+// eigenvalues ascending (solver.py:389, 622-626).
+constexpr int kEigWarps = 2;
+template <int NB>
+__global__ void __launch_bounds__(32 * kEigWarps, 8) k_cgr_eig(CgArgs a, const double2* __restrict__ A, int rotate,
+                                                            double tol) {
+  using RG = RowGroup<NB>;
+  constexpr int G = RG::G, KPW = RG::KPW, LP = RG::LP, MAT = RG::MAT, NP = JacobiPairs<NB>::M / 2;
+  __shared__ double2 st[kEigWarps][KPW][3 * MAT + 2 * NP];
+  __shared__ double sw[kEigWarps][KPW][NB];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, g = lane / G, c = lane % G;
+  double2* SQ = st[w][g];
+  double2* SA = SQ + MAT;
+  double2* SV = SA + MAT;
+  double2* SP = SV + MAT;
+  double* SW = sw[w][g];
+  for (int kb = (blockIdx.x * kEigWarps + w) * KPW; kb < a.nk; kb += gridDim.x * kEigWarps * KPW) {
+    const int k = kb + g;
+    const bool on = k < a.nk && c < NB;
+    const size_t base = (size_t)k * NB * NB + c;
+    if (on) {
+#pragma unroll
+      for (int r = 0; r < NB; ++r) SA[r * LP + c] = A[base + (size_t)r * NB];
+    }
+    if (rotate) {  // SA <- Q^H F Q, column c
+      double2 q[NB], m[NB];
+      if (on) {
+#pragma unroll
+        for (int r = 0; r < NB; ++r) {
+          q[r] = a.Q[base + (size_t)r * NB];
+          SQ[r * LP + c] = q[r];
+        }
+      }
+      __syncwarp();
+      if (on) {
+        double2 t[NB];
+#pragma unroll
+        for (int r = 0; r < NB; ++r) {
+          double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+          for (int j = 0; j < NB; ++j) acc = cfma(SA[r * LP + j], q[j], acc);
+          t[r] = acc;
+        }
+#pragma unroll
+        for (int i = 0; i < NB; ++i) {
+          double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+          for (int r = 0; r < NB; ++r) acc = cfma_cj(SQ[r * LP + i], t[r], acc);
+          m[i] = acc;
+        }
+      }
+      __syncwarp();
+      if (on) {
+#pragma unroll
+        for (int r = 0; r < NB; ++r) SA[r * LP + c] = m[r];
+      }
+    }
+    __syncwarp();
+    // hermitise (jnp.linalg.eigh symmetrises its input); V = I; Frobenius norm of the group
+    double2 hm[NB];
+    double fro = 0.0;
+    if (on) {
+#pragma unroll
+      for (int r = 0; r < NB; ++r) {
+        const double2 x = SA[r * LP + c], y = SA[c * LP + r];
+        hm[r] = r == c ? make_double2(x.x, 0.0) : make_double2(0.5 * (x.x + y.x), 0.5 * (x.y - y.y));
+        fro += hm[r].x * hm[r].x + hm[r].y * hm[r].y;
+      }
+    }
+#pragma unroll
+    for (int off = G / 2; off > 0; off >>= 1) fro += __shfl_xor_sync(0xffffffffu, fro, off);
+    __syncwarp();
+    if (on) {
+#pragma unroll
+      for (int r = 0; r < NB; ++r) {
+        SA[r * LP + c] = hm[r];
+        SV[r * LP + c] = make_double2(r == c ? 1.0 : 0.0, 0.0);
+      }
+    }
+    __syncwarp();
+    jacobi_smem_cols<NB>(SA, SV, SP, c, on, fmax(tol * sqrt(fro), 1e-300));
+    // ascending order: lane c's eigenpair goes to column rank(c)
+    const double wc = on ? SA[c * LP + c].x : 0.0;
+    if (on) SW[c] = wc;
+    __syncwarp();
+    if (on) {
+      int rk = 0;
+#pragma unroll
+      for (int j = 0; j < NB; ++j) rk += (SW[j] < wc) || (SW[j] == wc && j < c);
+      a.eps[(size_t)k * NB + rk] = wc;
+      const size_t out = (size_t)k * NB * NB + rk;
+      if (rotate) {  // (Q V)[r][rk] = sum_j Q[r][j] V[j][c]
+#pragma unroll
+        for (int r = 0; r < NB; ++r) {
+          double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+          for (int j = 0; j < NB; ++j) acc = cfma(SQ[r * LP + j], SV[j * LP + c], acc);
+          a.Q[out + (size_t)r * NB] = acc;
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < NB; ++r) a.Q[out + (size_t)r * NB] = SV[r * LP + c];
+      }
+    }
+    __syncwarp();
+  }
+}
+
 }  // namespace hf

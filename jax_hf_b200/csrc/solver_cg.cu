@@ -805,8 +805,24 @@ static int cg_density(CgRun& r, cudaStream_t s, int force) {
   return HF_OK;
 }
 
+template <int NB>
+static int cg_eig_rows(CgRun& r, cudaStream_t s, const double2* A, int rotate) {
+  const int per_block = kEigWarps * RowGroup<NB>::KPW;
+  int b = (r.a.nk + per_block - 1) / per_block;
+  if (b > 148 * 32) b = 148 * 32;
+  k_cgr_eig<NB><<<b < 1 ? 1 : b, 32 * kEigWarps, 0, s>>>(r.a, A, rotate, kEigTol);
+  HF_LAUNCH_CHECK("k_cgr_eig");
+  return HF_OK;
+}
+
 // eps, Q <- eigh(A) (init) or eigh(Q^H F Q) with Q <- Q V (finalize)
 static int cg_eig(CgRun& r, cudaStream_t s, const double2* A, int rotate) {
+  switch (r.a.nb) {
+#define HF_NB_CASE(N) case N: return cg_eig_rows<N>(r, s, A, rotate);
+    HF_NB_CASE(1) HF_NB_CASE(2) HF_NB_CASE(3) HF_NB_CASE(4) HF_NB_CASE(5) HF_NB_CASE(6) HF_NB_CASE(7) HF_NB_CASE(8)
+#undef HF_NB_CASE
+    default: break;
+  }
   const int nb = r.a.nb;
   k_cg_eig<<<r.nblk, 32 * kSolverWarps, smem_eig(nb), s>>>(r.a, A, rotate);
   HF_LAUNCH_CHECK("k_cg_eig");
