@@ -6,7 +6,7 @@ other frameworks' dispatchers) can call the CUDA kernels by name.  Each op has a
 fake (meta) implementation for shape propagation and an autograd formula that
 runs the hand-written adjoints of ``adjoint.py`` / ``csrc/adjoint.cu``:
 
-* ``hf_b200::fock_build(P, h, VR, include_exchange, include_hartree, packing)``
+* ``hf_b200::fock_build(P, h, VR, include_exchange, packing)``
   -> (Sigma, H, F), the interface of build_fock (fock.py:18-97) without refP,
   Hartree matrix or contact terms (use ``jax_hf_b200.build_fock`` for those);
   differentiable in P and h.
