@@ -5,8 +5,7 @@
 // unrolling).  Composite N = A*B is split Cooley-Tukey style: A-point DFTs over
 // x[n2 + B n1], the twiddle W_N^{n2 k1}, B-point DFTs, output X[k1 + A k2].
 // Radices 2/3/4/5/8 are the butterflies of fft_engine.cuh; other primes use a
-// direct DFT.  Twiddles come from a shared-memory table tw[e] = W_TWN^e of the
-// enclosing line length TWN (N divides TWN), so every index is a constant.
+// direct DFT.  Inner twiddles are compile-time constants (CtTwiddle).
 //
 // Line FFT of length N = N1*N2 over TPL threads per line (TPL | N1, TPL | N2):
 //   pattern A: thread t holds x[n2 + N2 n1] for n2 = t + TPL i (i < N2/TPL), all n1
@@ -16,6 +15,8 @@
 // inverse that starts from pattern B (N2-point IDFTs, twiddle, exchange,
 // N1-point IDFTs), so the spectrum never needs reordering between a forward
 // and an inverse transform.  Each call has one exchange; buf is [N][16] slots.
+// The runtime twiddles of a thread (they depend on t) come from its own row of
+// a shared-memory table (build_line_twiddles), indexed by compile-time offsets.
 #pragma once
 
 #include <utility>
@@ -173,13 +174,32 @@ struct LineShape {
   static constexpr int E1 = N2 / TPL;  // step-1 DFTs per thread
   static constexpr int E2 = N1 / TPL;  // step-2 DFTs per thread
   static constexpr int E = N / TPL;    // elements per thread
+  static constexpr int TS = E + 1;     // twiddle-row stride (odd in 16-byte units: no bank conflicts)
   static_assert(N1 * N2 == N && N2 % TPL == 0 && N1 % TPL == 0, "bad line shape");
   // index of element (i, n1) of pattern A and (j, k2) of pattern B
   __device__ static __forceinline__ int idxA(int t, int i, int n1) { return t + TPL * i + N2 * n1; }
   __device__ static __forceinline__ int idxB(int t, int j, int k2) { return t + TPL * j + N1 * k2; }
 };
 
-// pattern A -> pattern B (forward).  x[i*N1 + n1] in, x[j*N2 + k2] out.
+// Per-thread twiddle rows of a line shape: the step-1 twiddles W_N^{n2 k1} of
+// part t (n2 = t + TPL i) at twf[t TS + i N1 + k1], and the inverse-step
+// twiddles W_N^{k1 m2} (k1 = t + TPL j) at twi[t TS + j N2 + m2].  Each table
+// holds TPL * TS entries; values are those of exp(-2 pi i e / N) from sincospi.
+template <class S, typename T>
+__device__ __forceinline__ void build_line_twiddles(cpx_t<T>* twf, cpx_t<T>* twi) {
+  for (int q = threadIdx.x; q < S::TPL * S::E; q += blockDim.x) {
+    const int t = q / S::E, r = q - t * S::E;
+    const int ef = ((t + S::TPL * (r / S::N1)) * (r % S::N1)) % S::N;
+    const int ei = ((t + S::TPL * (r / S::N2)) * (r % S::N2)) % S::N;
+    double sn, cs;
+    sincospi(-2.0 * (double)ef / (double)S::N, &sn, &cs);
+    twf[t * S::TS + r] = mk<cpx_t<T>>(cs, sn);
+    sincospi(-2.0 * (double)ei / (double)S::N, &sn, &cs);
+    twi[t * S::TS + r] = mk<cpx_t<T>>(cs, sn);
+  }
+}
+
+// pattern A -> pattern B (forward).  tw = this thread's row of twf.  x[i*N1 + n1] in, x[j*N2 + k2] out.
 template <class S, typename C>
 __device__ __forceinline__ void fwd_AB(C* x, C* __restrict__ buf, const C* __restrict__ tw, int t, int s) {
 #pragma unroll
@@ -189,7 +209,7 @@ __device__ __forceinline__ void fwd_AB(C* x, C* __restrict__ buf, const C* __res
 #pragma unroll
     for (int k1 = 0; k1 < S::N1; ++k1) {
       C v = x[i * S::N1 + k1];
-      if (k1 != 0) v = cmul(v, tw[(n2 * k1) % S::N]);
+      if (k1 != 0) v = cmul(v, tw[i * S::N1 + k1]);
       buf[(k1 * S::N2 + n2) * 16 + s] = v;
     }
   }
@@ -204,18 +224,23 @@ __device__ __forceinline__ void fwd_AB(C* x, C* __restrict__ buf, const C* __res
 }
 
 // pattern B -> pattern A (inverse, unnormalised).  x[j*N2 + k2] in, x[i*N1 + m1] out.
-template <class S, typename C>
-__device__ __forceinline__ void inv_BA(C* x, C* __restrict__ buf, const C* __restrict__ tw, int t, int s) {
+// tw = this thread's row of twi (applied conjugated; the k1 = 0 row is all ones).
+// pre() runs after the N2-point IDFTs (registers only) and before the first
+// write to buf, e.g. a wait until buf may be overwritten.
+template <class S, typename C, typename Pre>
+__device__ __forceinline__ void inv_BA(C* x, C* __restrict__ buf, const C* __restrict__ tw, int t, int s, Pre pre) {
 #pragma unroll
   for (int j = 0; j < S::E2; ++j) {
     rdft<S::N2, S::N, true>(x + j * S::N2, tw);
+#pragma unroll
+    for (int m2 = 1; m2 < S::N2; ++m2) x[j * S::N2 + m2] = cmulc(x[j * S::N2 + m2], tw[j * S::N2 + m2]);
+  }
+  pre();
+#pragma unroll
+  for (int j = 0; j < S::E2; ++j) {
     const int k1 = t + S::TPL * j;
 #pragma unroll
-    for (int m2 = 0; m2 < S::N2; ++m2) {
-      C v = x[j * S::N2 + m2];
-      if (m2 != 0 && k1 != 0) v = cmulc(v, tw[(k1 * m2) % S::N]);
-      buf[(k1 * S::N2 + m2) * 16 + s] = v;
-    }
+    for (int m2 = 0; m2 < S::N2; ++m2) buf[(k1 * S::N2 + m2) * 16 + s] = x[j * S::N2 + m2];
   }
   __syncthreads();
 #pragma unroll
@@ -225,6 +250,10 @@ __device__ __forceinline__ void inv_BA(C* x, C* __restrict__ buf, const C* __res
     for (int k1 = 0; k1 < S::N1; ++k1) x[i * S::N1 + k1] = buf[(k1 * S::N2 + m2) * 16 + s];
     rdft<S::N1, S::N, true>(x + i * S::N1, tw);
   }
+}
+template <class S, typename C>
+__device__ __forceinline__ void inv_BA(C* x, C* __restrict__ buf, const C* __restrict__ tw, int t, int s) {
+  inv_BA<S>(x, buf, tw, t, s, [] {});
 }
 
 }  // namespace hf

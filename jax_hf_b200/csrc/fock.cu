@@ -29,6 +29,7 @@ namespace hf {
 // ------------------------------------------------------------ planning -----
 struct SlotPlan {
   int LS = 0, ngroups = 0;
+  bool rows = false;  // rows plan of the fast passes (plan_rows)
   std::vector<int16_t> chan, partner;
 };
 
@@ -420,8 +421,30 @@ static size_t fft_elem(int dtype, unsigned flags) {
   return (dtype == HF_C64 || (flags & HF_FOCK_FFT_FP32)) ? sizeof(float2) : sizeof(double2);
 }
 
+// Rows plan for the fast passes (nb <= 8, no packing): group g holds the whole
+// matrix rows [g R, g R + R), R = min(nb, 16 / nb), LS = R nb slots, so every
+// k-point's channels of a group are contiguous in memory; the herm partner
+// (b, a) of slot (a, b) is in group b / R: partner = (group << 8) | slot.
+static void plan_rows(int nb, SlotPlan& out) {
+  const int R = std::min(nb, 16 / nb);
+  out.rows = true;
+  out.LS = R * nb;
+  out.ngroups = (nb + R - 1) / R;
+  out.chan.assign(out.LS * out.ngroups, -1);
+  out.partner.assign(out.LS * out.ngroups, -1);
+  for (int c = 0; c < nb * nb; ++c) {
+    const int a = c / nb, b = c % nb, cp = b * nb + a, gp = b / R;
+    out.chan[c] = (int16_t)c;
+    out.partner[c] = (int16_t)((gp << 8) | (cp - gp * out.LS));
+  }
+}
+
 static int get_plan(int dtype, unsigned flags, int nk1, int nk2, int nb, SlotPlan& sp) {
   const bool packing = (flags & HF_FOCK_PACKING) != 0;
+  if (!packing && nb <= 8 && !(flags & HF_FOCK_GENERIC_FFT) && fast_length(nk1) && fast_length(nk2)) {
+    plan_rows(nb, sp);
+    return HF_OK;
+  }
   const int max_ls = (fast_length(nk1) && fast_length(nk2)) ? 16 : 32;
   int st = plan_slots(nb, packing, std::max(nk1, nk2), fft_elem(dtype, flags), max_ls, sp);
   if (st != HF_OK) return fail(st, "mesh too large for the shared-memory FFT (nk1, nk2 <= 768 in complex128)");
@@ -517,7 +540,7 @@ int hf::fock_build_internal(void* stream, int dtype, unsigned flags, int nk1, in
   FockParams p;
   memset(&p, 0, sizeof(p));
   p.nk1 = nk1; p.nk2 = nk2; p.nb = nb; p.nb2 = nb * nb;
-  p.LS = sp.LS; p.ngroups = sp.ngroups;
+  p.LS = sp.LS; p.ngroups = sp.ngroups; p.rows_plan = sp.rows ? 1 : 0;
   p.flags = flags; p.n_contact = n_contact;
   p.scale = -1.0 / ((double)nk1 * (double)nk2);
   p.row = make_fft_plan(nk2);

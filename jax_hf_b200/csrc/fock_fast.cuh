@@ -12,7 +12,13 @@
 //   col     : scratch column (pattern A along k1) -> FFT -> x(-VR/N) -> IFFT -> scratch
 //   row_inv : scratch (pattern B) -> IFFT -> epilogue (contact, Hartree, herm via a
 //             lane shuffle with the transposed channel, + h) -> Sigma, F
+// With the rows plan (nb <= 8, no packing) a slot group holds whole matrix rows,
+// so the P, h, Sigma and F accesses of a k-point are contiguous, and the inverse
+// row pass runs as clusters of ngroups CTAs that exchange the herm partners
+// through distributed shared memory (k_fast_row_inv_rows).
 #pragma once
+
+#include <cooperative_groups.h>
 
 #include "fft_reg.cuh"
 #include "fock_params.cuh"
@@ -40,6 +46,42 @@ __device__ __forceinline__ void cp_async8(void* dst, const void* src, bool valid
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
+// Programmatic dependent launch: the column and inverse row passes are launched
+// with programmatic stream serialization, so their CTAs may start (twiddle
+// tables, index setup) while the previous pass finishes; pdl_wait()
+// (griddepcontrol.wait: the previous grid has completed and its writes are
+// visible) comes before the first read of anything an earlier kernel wrote.
+// Without the launch attribute griddepcontrol.wait returns at once.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+
+// Launches kernel<<<grid, block, smem, stream>>>(p) with programmatic stream
+// serialization (and a cluster shape when csize > 0).
+template <typename K>
+inline cudaError_t launch_pass(K kernel, int grid, int block, size_t smem, cudaStream_t stream, const FockParams& p,
+                               int csize = 0) {
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[2];
+  int na = 0;
+  attr[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[na].val.programmaticStreamSerializationAllowed = 1;
+  ++na;
+  if (csize > 0) {
+    attr[na].id = cudaLaunchAttributeClusterDimension;
+    attr[na].val.clusterDim.x = (unsigned)csize;
+    attr[na].val.clusterDim.y = 1;
+    attr[na].val.clusterDim.z = 1;
+    ++na;
+  }
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cfg.attrs = attr;
+  cfg.numAttrs = na;
+  return cudaLaunchKernelEx(&cfg, kernel, p);
+}
+
 // Each fast pass is a persistent kernel: CTA b handles items b, b + grid, ...
 // (item = slot group g + ngroups * line), and while it transforms one item the
 // copies of the next one are already in flight into `stage`.  Every thread
@@ -66,16 +108,18 @@ __device__ __forceinline__ void stage_row_fwd(const FockParams& p, cpx_t<FT>* st
 template <typename ST, typename FT, class S>
 __global__ void __launch_bounds__(16 * S::TPL) k_fast_row_fwd(const __grid_constant__ FockParams p) {
   if (p.active && !*p.active) return;
+  pdl_launch_dependents();
   using SC = cpx_t<ST>;
   using FC = cpx_t<FT>;
   constexpr bool kStage = sizeof(SC) == sizeof(FC);  // mixed precision converts in registers
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  FC* tw = reinterpret_cast<FC*>(smem_raw);
-  FC* buf = tw + S::N;
+  FC* twf = reinterpret_cast<FC*>(smem_raw);
+  FC* twi = twf + S::TPL * S::TS;
+  FC* buf = twi + S::TPL * S::TS;
   FC* stage = buf + 16 * S::N;
   const int t = threadIdx.x >> 4, s = threadIdx.x & 15, LS = p.LS;
   const int nitems = p.ngroups * p.nk1;
-  build_twiddles<FT>(tw, S::N);
+  build_line_twiddles<S, FT>(twf, twi);
   const bool has_ref = (p.flags & HF_FOCK_HAS_REFP) != 0;
   int item = blockIdx.x;
   if (kStage && item < nitems) {
@@ -114,7 +158,7 @@ __global__ void __launch_bounds__(16 * S::TPL) k_fast_row_fwd(const __grid_const
         for (int n1 = 0; n1 < S::N1; ++n1)
           x[i * S::N1 + n1] = csub(x[i * S::N1 + n1], cvt<FC>(ld_stream(R + (size_t)S::idxA(t, i, n1) * p.nb2)));
     }
-    fwd_AB<S>(x, buf, tw, t, s);
+    fwd_AB<S>(x, buf, twf + t * S::TS, t, s);
     if (s < LS) {
       FC* out = static_cast<FC*>(p.scratch) + ((size_t)g * p.nk1 + k1) * S::N * LS + s;
 #pragma unroll
@@ -145,21 +189,24 @@ __device__ __forceinline__ void stage_col(const FockParams& p, cpx_t<FT>* stage,
 
 template <typename ST, typename FT, class S>
 __global__ void __launch_bounds__(16 * S::TPL, 2) k_fast_col(const __grid_constant__ FockParams p) {
-  if (p.active && !*p.active) return;
+  pdl_launch_dependents();
   using SC = cpx_t<ST>;
   using FC = cpx_t<FT>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  FC* tw = reinterpret_cast<FC*>(smem_raw);
-  FC* buf = tw + S::N;
+  FC* twf = reinterpret_cast<FC*>(smem_raw);
+  FC* twi = twf + S::TPL * S::TS;
+  FC* buf = twi + S::TPL * S::TS;
   FC* stage = buf + 16 * S::N;
   const int t = threadIdx.x >> 4, s = threadIdx.x & 15, LS = p.LS;
   const int nitems = p.ngroups * p.nk2;
-  build_twiddles<FT>(tw, S::N);
+  build_line_twiddles<S, FT>(twf, twi);
   const bool vr_scalar = (p.flags & HF_FOCK_VR_SCALAR) != 0;
   const bool vr_real = (p.flags & HF_FOCK_VR_REAL) != 0;
   const size_t vstride = vr_scalar ? 1 : (size_t)p.nb2;
   const size_t rs = (size_t)p.nk2 * LS;
   int item = blockIdx.x;
+  pdl_wait();  // the row pass has finished writing the scratch
+  if (p.active && !*p.active) return;
   if (item < nitems) stage_col<FT, S>(p, stage, item % p.ngroups, item / p.ngroups, t, s);
   __syncthreads();
   for (; item < nitems; item += gridDim.x) {
@@ -190,14 +237,14 @@ __global__ void __launch_bounds__(16 * S::TPL, 2) k_fast_col(const __grid_consta
       for (int n1 = 0; n1 < S::N1; ++n1) x[i * S::N1 + n1] = stage[S::idxA(t, i, n1) * 16 + s];
     const int nx = item + gridDim.x;
     if (nx < nitems) stage_col<FT, S>(p, stage, nx % p.ngroups, nx / p.ngroups, t, s);
-    fwd_AB<S>(x, buf, tw, t, s);
+    fwd_AB<S>(x, buf, twf + t * S::TS, t, s);
 #pragma unroll
     for (int e = 0; e < S::E; ++e) {
       FC v = x[e];
       x[e] = c < 0 ? mk<FC>(0.0, 0.0) : mk<FC>(v.x * vr[e] - v.y * vi[e], v.x * vi[e] + v.y * vr[e]);
     }
     __syncthreads();  // buf is reused by the inverse transform
-    inv_BA<S>(x, buf, tw, t, s);
+    inv_BA<S>(x, buf, twi + t * S::TS, t, s);
     if (s < LS) {
       FC* col = static_cast<FC*>(p.scratch) + ((size_t)g * p.nk1 * p.nk2 + k2c) * LS + s;
 #pragma unroll
@@ -227,12 +274,12 @@ __device__ __forceinline__ void stage_row_inv(const FockParams& p, cpx_t<FT>* st
 
 template <typename ST, typename FT, class S>
 __global__ void __launch_bounds__(16 * S::TPL, 2) k_fast_row_inv(const __grid_constant__ FockParams p) {
-  if (p.active && !*p.active) return;
   using SC = cpx_t<ST>;
   using FC = cpx_t<FT>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  FC* tw = reinterpret_cast<FC*>(smem_raw);
-  FC* buf = tw + S::N;
+  FC* twf = reinterpret_cast<FC*>(smem_raw);
+  FC* twi = twf + S::TPL * S::TS;
+  FC* buf = twi + S::TPL * S::TS;
   FC* stage = buf + 16 * S::N;
   const int t = threadIdx.x >> 4, s = threadIdx.x & 15;
   const int lane = threadIdx.x & 31;
@@ -244,8 +291,10 @@ __global__ void __launch_bounds__(16 * S::TPL, 2) k_fast_row_inv(const __grid_co
   const SC* h = static_cast<const SC*>(p.h);
   SC* Sg = static_cast<SC*>(p.Sigma);
   SC* F = static_cast<SC*>(p.F);
-  build_twiddles<FT>(tw, S::N);
+  build_line_twiddles<S, FT>(twf, twi);
   int item = blockIdx.x;
+  pdl_wait();  // the column pass has finished writing the scratch
+  if (p.active && !*p.active) return;
   if (exch && item < nitems) stage_row_inv<FT, S>(p, stage, item % p.ngroups, item / p.ngroups, t, s);
   __syncthreads();
   for (; item < nitems; item += gridDim.x) {
@@ -271,7 +320,7 @@ __global__ void __launch_bounds__(16 * S::TPL, 2) k_fast_row_inv(const __grid_co
         for (int k2 = 0; k2 < S::N2; ++k2) x[j * S::N2 + k2] = stage[S::idxB(t, j, k2) * 16 + s];
       const int nx = item + gridDim.x;
       if (nx < nitems) stage_row_inv<FT, S>(p, stage, nx % p.ngroups, nx / p.ngroups, t, s);
-      inv_BA<S>(x, buf, tw, t, s);
+      inv_BA<S>(x, buf, twi + t * S::TS, t, s);
     } else {
 #pragma unroll
       for (int e = 0; e < S::E; ++e) x[e] = mk<FC>(0.0, 0.0);
@@ -317,9 +366,122 @@ __global__ void __launch_bounds__(16 * S::TPL, 2) k_fast_row_inv(const __grid_co
   }
 }
 
+// Cluster barrier halves (all threads of every CTA of the cluster take part).
+__device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory"); }
+__device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory"); }
+
+// Inverse row pass of the rows plan (see the file comment).  Cluster q of the
+// grid takes rows k1 = q, q + nclusters, ...; CTA rank g of the cluster is slot
+// group g.  Per row: inverse FFT of the group's spectrum row (direct L2 loads,
+// no stage; 2 CTAs per SM without register spills), Sigma = result + contact, M = h + Sigma into shared
+// memory, cluster barrier A, F = (M + M_partner^H) / 2 + Hartree with M_partner
+// read from the partner group's CTA (partner = (group << 8) | slot), arrival at
+// cluster barrier B.  The wait on B (the partners have read the buffer) comes
+// in the next row after its loads and first FFT step, just before the buffer
+// is overwritten, and once more before the CTA exits.
+template <typename ST, typename FT, class S>
+__global__ void __launch_bounds__(16 * S::TPL, 2) k_fast_row_inv_rows(const __grid_constant__ FockParams p) {
+  namespace cg = cooperative_groups;
+  using SC = cpx_t<ST>;
+  using FC = cpx_t<FT>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  FC* twf = reinterpret_cast<FC*>(smem_raw);
+  FC* twi = twf + S::TPL * S::TS;
+  FC* buf = twi + S::TPL * S::TS;  // FFT exchange, then M
+  SC* mbuf = reinterpret_cast<SC*>(buf);
+  cg::cluster_group cluster = cg::this_cluster();
+  const int g = (int)cluster.block_rank();
+  const int ncl = gridDim.x / p.ngroups, cl = blockIdx.x / p.ngroups;
+  const int t = threadIdx.x >> 4, s = threadIdx.x & 15;
+  const int LS = p.LS, nb = p.nb;
+  const bool exch = (p.flags & HF_FOCK_EXCHANGE) != 0;
+  const SC* h = static_cast<const SC*>(p.h);
+  SC* Sg = static_cast<SC*>(p.Sigma);
+  SC* F = static_cast<SC*>(p.F);
+  build_line_twiddles<S, FT>(twf, twi);
+  const int c = s < LS ? p.chan[g * LS + s] : -1;
+  const int pe = c >= 0 ? p.partner[g * LS + s] : ((g << 8) | s);
+  const SC* pbuf = cluster.map_shared_rank(mbuf, pe >> 8) + (pe & 255);
+  pdl_wait();  // scratch, contact sigma and Hartree diagonal come from earlier kernels
+  if (p.active && !*p.active) return;  // the flag is uniform over the grid
+  const int cc = c >= 0 ? c : 0;
+  SC cab = mk<SC>(0.0, 0.0);
+  double hd = 0.0;
+  if (p.sigc != nullptr && c >= 0) {
+    cab = cvt<SC>(p.sigc[c]);
+    if (cc / nb == cc % nb) hd = p.hdiag[cc / nb];
+  }
+  __syncthreads();
+  bool pending = false;  // arrived at barrier B, not yet waited
+  for (int k1 = cl; k1 < p.nk1; k1 += ncl) {
+    const size_t base = ((size_t)k1 * S::N + t) * p.nb2 + cc;
+    // h for this thread's k-points, issued before the transform
+    SC m[S::E];
+#pragma unroll
+    for (int i = 0; i < S::E1; ++i)
+#pragma unroll
+      for (int m1 = 0; m1 < S::N1; ++m1)
+        m[i * S::N1 + m1] = c >= 0 ? ld_stream(h + base + (size_t)(S::TPL * i + S::N2 * m1) * p.nb2) : mk<SC>(0.0, 0.0);
+    FC x[S::E];
+    if (exch) {
+      const FC* rowp = static_cast<const FC*>(p.scratch) + ((size_t)g * p.nk1 + k1) * S::N * LS + (s < LS ? s : 0);
+#pragma unroll
+      for (int j = 0; j < S::E2; ++j)
+#pragma unroll
+        for (int k2 = 0; k2 < S::N2; ++k2)
+          x[j * S::N2 + k2] = s < LS ? __ldcg(rowp + S::idxB(t, j, k2) * LS) : mk<FC>(0.0, 0.0);
+      inv_BA<S>(x, buf, twi + t * S::TS, t, s, [&] {
+        if (pending) cluster_wait();
+        pending = false;
+      });
+    } else {
+#pragma unroll
+      for (int e = 0; e < S::E; ++e) x[e] = mk<FC>(0.0, 0.0);
+      if (pending) cluster_wait();
+      pending = false;
+    }
+    __syncthreads();  // the exchange reads of buf are done: it now takes M
+#pragma unroll
+    for (int i = 0; i < S::E1; ++i)
+#pragma unroll
+      for (int m1 = 0; m1 < S::N1; ++m1) {
+        const int e = i * S::N1 + m1;
+        const SC sab = cadd(cvt<SC>(x[e]), cab);
+        m[e] = cadd(m[e], sab);
+        mbuf[S::idxA(t, i, m1) * 16 + s] = m[e];
+      }
+    cluster_arrive();  // barrier A: M of every group is in shared memory
+#pragma unroll
+    for (int i = 0; i < S::E1; ++i)
+#pragma unroll
+      for (int m1 = 0; m1 < S::N1; ++m1)
+        if (c >= 0) st_stream(Sg + base + (size_t)(S::TPL * i + S::N2 * m1) * p.nb2, cadd(cvt<SC>(x[i * S::N1 + m1]), cab));
+    cluster_wait();
+#pragma unroll
+    for (int i = 0; i < S::E1; ++i)
+#pragma unroll
+      for (int m1 = 0; m1 < S::N1; ++m1) {
+        const int e = i * S::N1 + m1;
+        const SC mo = pbuf[S::idxA(t, i, m1) * 16];
+        if (c >= 0)
+          st_stream(F + base + (size_t)(S::TPL * i + S::N2 * m1) * p.nb2,
+                    mk<SC>(0.5 * ((double)m[e].x + (double)mo.x) + hd, 0.5 * ((double)m[e].y - (double)mo.y)));
+      }
+    cluster_arrive();  // barrier B: this CTA's reads of the partners' buffers are done
+    pending = true;
+  }
+  if (pending) cluster_wait();  // no CTA exits while a partner may read its buffer
+}
+
 template <class S, typename FT>
 constexpr size_t fast_smem() {
-  return (size_t)(S::N + 32 * S::N) * sizeof(cpx_t<FT>);  // twiddles, exchange buffer, stage
+  return (size_t)(2 * S::TPL * S::TS + 32 * S::N) * sizeof(cpx_t<FT>);  // twiddle rows, exchange buffer, stage
+}
+// k_fast_row_inv_rows: twiddle rows and one buffer of 16 N entries (FFT exchange, then M)
+template <class S, typename ST, typename FT>
+constexpr size_t fast_smem_rows() {
+  constexpr size_t e = sizeof(cpx_t<ST>) > sizeof(cpx_t<FT>) ? sizeof(cpx_t<ST>) : sizeof(cpx_t<FT>);
+  return (size_t)(2 * S::TPL * S::TS) * sizeof(cpx_t<FT>) + 16 * (size_t)S::N * e;
 }
 
 // Persistent grid: CTAs resident on the device (2 per SM for the large shapes).
@@ -356,14 +518,39 @@ int fast_fock(FockParams& p, cudaStream_t stream, bool* handled) {
     constexpr size_t sm = fast_smem<S, FT>();
     cudaFuncSetAttribute(k_fast_col<ST, FT, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     const int grid = persistent_grid(k_fast_col<ST, FT, S>, 16 * S::TPL, sm, p.ngroups * p.nk2);
-    k_fast_col<ST, FT, S><<<grid, 16 * S::TPL, sm, stream>>>(p);
+    const cudaError_t e = launch_pass(k_fast_col<ST, FT, S>, grid, 16 * S::TPL, sm, stream, p);
+    if (e != cudaSuccess) st = cuda_check(e, "k_fast_col");
   };
   auto inv = [&](auto shape) {
     using S = decltype(shape);
+    if (p.rows_plan) {
+      constexpr size_t sm = fast_smem_rows<S, ST, FT>();
+      auto kern = k_fast_row_inv_rows<ST, FT, S>;
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      cudaLaunchConfig_t cfg = {};
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = (unsigned)p.ngroups;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.gridDim = dim3((unsigned)p.ngroups);
+      cfg.blockDim = dim3(16 * S::TPL);
+      cfg.dynamicSmemBytes = sm;
+      cfg.stream = stream;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      int ncl = 0;
+      if (cudaOccupancyMaxActiveClusters(&ncl, kern, &cfg) != cudaSuccess || ncl < 1) ncl = 1;
+      if (ncl > p.nk1) ncl = p.nk1;
+      const cudaError_t e = launch_pass(kern, ncl * p.ngroups, 16 * S::TPL, sm, stream, p, p.ngroups);
+      if (e != cudaSuccess) st = cuda_check(e, "k_fast_row_inv_rows");
+      return;
+    }
     constexpr size_t sm = fast_smem<S, FT>();
     cudaFuncSetAttribute(k_fast_row_inv<ST, FT, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     const int grid = persistent_grid(k_fast_row_inv<ST, FT, S>, 16 * S::TPL, sm, p.ngroups * p.nk1);
-    k_fast_row_inv<ST, FT, S><<<grid, 16 * S::TPL, sm, stream>>>(p);
+    const cudaError_t e = launch_pass(k_fast_row_inv<ST, FT, S>, grid, 16 * S::TPL, sm, stream, p);
+    if (e != cudaSuccess) st = cuda_check(e, "k_fast_row_inv");
   };
   switch (p.nk2) {
 #define HF_CASE(N, A, B, T) case N: row(LineShape<N, A, B, T>{}); break;

@@ -32,6 +32,7 @@ struct FockParams {
   double2* sigc;      // [nb*nb] contact sigma
   double* hdiag;      // [nb] Hartree diagonal
   const int* active;  // optional device flag: kernels return at once when *active == 0
+  int rows_plan;      // slot groups are whole matrix rows; partner = (group << 8) | slot
   int16_t chan[kMaxSlotTable];
   int16_t partner[kMaxSlotTable];
 };
