@@ -369,6 +369,13 @@ __global__ void __launch_bounds__(16 * S::TPL, 2) k_fast_row_inv(const __grid_co
 // Cluster barrier halves (all threads of every CTA of the cluster take part).
 __device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory"); }
 __device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory"); }
+// Arrival without release semantics, for a barrier that only says "my reads of
+// the other CTAs' shared memory are done" (their values have been consumed, so
+// no later write can change them); it does not wait for this thread's global
+// stores to complete, as a release would.
+__device__ __forceinline__ void cluster_arrive_relaxed() {
+  asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory");
+}
 
 // Inverse row pass of the rows plan (see the file comment).  Cluster q of the
 // grid takes rows k1 = q, q + nclusters, ...; CTA rank g of the cluster is slot
@@ -389,6 +396,7 @@ __global__ void __launch_bounds__(16 * S::TPL, 2) k_fast_row_inv_rows(const __gr
   FC* twi = twf + S::TPL * S::TS;
   FC* buf = twi + S::TPL * S::TS;  // FFT exchange, then M
   SC* mbuf = reinterpret_cast<SC*>(buf);
+  FC* stage = reinterpret_cast<FC*>(mbuf + 16 * S::N);  // cp.async stage of the next spectrum row
   cg::cluster_group cluster = cg::this_cluster();
   const int g = (int)cluster.block_rank();
   const int ncl = gridDim.x / p.ngroups, cl = blockIdx.x / p.ngroups;
@@ -411,6 +419,7 @@ __global__ void __launch_bounds__(16 * S::TPL, 2) k_fast_row_inv_rows(const __gr
     cab = cvt<SC>(p.sigc[c]);
     if (cc / nb == cc % nb) hd = p.hdiag[cc / nb];
   }
+  if (exch && cl < p.nk1) stage_row_inv<FT, S>(p, stage, g, cl, t, s);
   __syncthreads();
   bool pending = false;  // arrived at barrier B, not yet waited
   for (int k1 = cl; k1 < p.nk1; k1 += ncl) {
@@ -424,12 +433,12 @@ __global__ void __launch_bounds__(16 * S::TPL, 2) k_fast_row_inv_rows(const __gr
         m[i * S::N1 + m1] = c >= 0 ? ld_stream(h + base + (size_t)(S::TPL * i + S::N2 * m1) * p.nb2) : mk<SC>(0.0, 0.0);
     FC x[S::E];
     if (exch) {
-      const FC* rowp = static_cast<const FC*>(p.scratch) + ((size_t)g * p.nk1 + k1) * S::N * LS + (s < LS ? s : 0);
+      cp_async_wait_all();  // this thread's copies of the row (no barrier: it reads only what it copied)
 #pragma unroll
       for (int j = 0; j < S::E2; ++j)
 #pragma unroll
-        for (int k2 = 0; k2 < S::N2; ++k2)
-          x[j * S::N2 + k2] = s < LS ? __ldcg(rowp + S::idxB(t, j, k2) * LS) : mk<FC>(0.0, 0.0);
+        for (int k2 = 0; k2 < S::N2; ++k2) x[j * S::N2 + k2] = stage[S::idxB(t, j, k2) * 16 + s];
+      if (k1 + ncl < p.nk1) stage_row_inv<FT, S>(p, stage, g, k1 + ncl, t, s);
       inv_BA<S>(x, buf, twi + t * S::TS, t, s, [&] {
         if (pending) cluster_wait();
         pending = false;
@@ -467,7 +476,7 @@ __global__ void __launch_bounds__(16 * S::TPL, 2) k_fast_row_inv_rows(const __gr
           st_stream(F + base + (size_t)(S::TPL * i + S::N2 * m1) * p.nb2,
                     mk<SC>(0.5 * ((double)m[e].x + (double)mo.x) + hd, 0.5 * ((double)m[e].y - (double)mo.y)));
       }
-    cluster_arrive();  // barrier B: this CTA's reads of the partners' buffers are done
+    cluster_arrive_relaxed();  // barrier B: this CTA's reads of the partners' buffers are done
     pending = true;
   }
   if (pending) cluster_wait();  // no CTA exits while a partner may read its buffer
@@ -477,11 +486,11 @@ template <class S, typename FT>
 constexpr size_t fast_smem() {
   return (size_t)(2 * S::TPL * S::TS + 32 * S::N) * sizeof(cpx_t<FT>);  // twiddle rows, exchange buffer, stage
 }
-// k_fast_row_inv_rows: twiddle rows and one buffer of 16 N entries (FFT exchange, then M)
+// k_fast_row_inv_rows: twiddle rows, one buffer of 16 N entries (FFT exchange, then M), the stage
 template <class S, typename ST, typename FT>
 constexpr size_t fast_smem_rows() {
   constexpr size_t e = sizeof(cpx_t<ST>) > sizeof(cpx_t<FT>) ? sizeof(cpx_t<ST>) : sizeof(cpx_t<FT>);
-  return (size_t)(2 * S::TPL * S::TS) * sizeof(cpx_t<FT>) + 16 * (size_t)S::N * e;
+  return (size_t)(2 * S::TPL * S::TS) * sizeof(cpx_t<FT>) + 16 * (size_t)S::N * e + 16 * (size_t)S::N * sizeof(cpx_t<FT>);
 }
 
 // Persistent grid: CTAs resident on the device (2 per SM for the large shapes).
