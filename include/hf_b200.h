@@ -53,6 +53,10 @@ extern "C" {
  * upper-triangle channels are transformed, Sigma_ba = conj(Sigma_ab)); exact
  * for a Hermitian density.  The reference packs scalar V only (utils.py:140-161). */
 #define HF_FOCK_SYM_V (1u << 8)
+/* Use the transpose-closed 2x2-tile slot groups in the fast engine even where
+ * the rows plan would apply (nb <= 8 without packing); a schedule choice, the
+ * result is the same to rounding. */
+#define HF_FOCK_TILE_PLAN (1u << 9)
 const char* hf_last_error(void);
 const char* hf_status_string(int status);
 int hf_version(void);
@@ -96,6 +100,29 @@ int hf_fock_build_static_scratch(void* stream, int dtype, unsigned flags, int nk
                                  const void* HH, const void* w2d, int n_contact, const void* contact_g,
                                  const void* contact_Oi, const void* contact_Oj, void* Sigma, void* H,
                                  void* F);
+
+/* Autotuner for the Fock-build schedule (the north-star's "tile and radix
+ * schedules picked by an autotuner"; no counterpart in the reference, whose
+ * FFTs are XLA's).  Same arguments as hf_fock_build, plus reps (timed builds
+ * per candidate, >= 1), chosen (out: the engine flags picked) and us (out,
+ * may be NULL: mean microseconds per build of each candidate, in the order
+ * default schedule / HF_FOCK_TILE_PLAN / HF_FOCK_GENERIC_FFT, -1 for a
+ * candidate that does not apply).  Every candidate runs on the caller's
+ * buffers (one untimed build, then reps timed with CUDA events on `stream`),
+ * the fastest is stored in a process-wide table keyed by (device, dtype,
+ * flags, nk1, nk2, nb), and the outputs hold the winner's result on return.
+ * Later hf_fock_build calls with the same key and no engine flag of their own
+ * (HF_FOCK_TILE_PLAN, HF_FOCK_GENERIC_FFT), including those made inside the
+ * solver drivers, use the stored choice.  Synchronises `stream`: call it
+ * outside stream capture.  The workspace must hold
+ * hf_fock_workspace_size(), which covers every candidate. */
+int hf_fock_autotune(void* stream, int dtype, unsigned flags, int nk1, int nk2, int nb, const void* P,
+                     const void* h, const void* VR, const void* refP, const void* HH, const void* w2d,
+                     int n_contact, const void* contact_g, const void* contact_Oi, const void* contact_Oj,
+                     void* Sigma, void* H, void* F, void* workspace, size_t workspace_bytes, int reps,
+                     unsigned* chosen, float* us);
+/* Forgets every stored autotuner choice. */
+int hf_fock_autotune_reset(void);
 
 /* ---- Objective reductions (compensated, FP64 accumulation) -----------------
  * hf_energy replaces fock.hf_energy (fock.py:100-111):

@@ -30,6 +30,7 @@ FOCK_FFT_FP32 = 1 << 5
 FOCK_HAS_REFP = 1 << 6
 FOCK_GENERIC_FFT = 1 << 7
 FOCK_SYM_V = 1 << 8
+FOCK_TILE_PLAN = 1 << 9
 
 vp, i32, u32, f64, sz = C.c_void_p, C.c_int, C.c_uint, C.c_double, C.c_size_t
 pf64 = C.POINTER(C.c_double)
@@ -42,6 +43,9 @@ _SIGS = {
     "hf_fock_workspace_size": ([i32, u32, i32, i32, i32, psz], i32),
     "hf_fock_build": ([vp, i32, u32, i32, i32, i32, vp, vp, vp, vp, vp, vp, i32, vp, vp, vp,
                        vp, vp, vp, vp, sz], i32),
+    "hf_fock_autotune": ([vp, i32, u32, i32, i32, i32, vp, vp, vp, vp, vp, vp, i32, vp, vp, vp,
+                          vp, vp, vp, vp, sz, i32, C.POINTER(C.c_uint), C.POINTER(C.c_float)], i32),
+    "hf_fock_autotune_reset": ([], i32),
     "hf_fock_build_static_scratch": ([vp, i32, u32, i32, i32, i32, vp, vp, vp, vp, vp, vp, i32, vp, vp, vp,
                                       vp, vp, vp], i32),
     "hf_reduce_workspace_size": ([i32, i32, i32, psz], i32),

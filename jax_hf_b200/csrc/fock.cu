@@ -17,7 +17,9 @@
 // F needs no extra pass, and each 2x2 tile keeps 32-byte sectors whole.
 #include <algorithm>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "common.cuh"
@@ -441,7 +443,8 @@ static void plan_rows(int nb, SlotPlan& out) {
 
 static int get_plan(int dtype, unsigned flags, int nk1, int nk2, int nb, SlotPlan& sp) {
   const bool packing = (flags & HF_FOCK_PACKING) != 0;
-  if (!packing && nb <= 8 && !(flags & HF_FOCK_GENERIC_FFT) && fast_length(nk1) && fast_length(nk2)) {
+  if (!packing && nb <= 8 && !(flags & (HF_FOCK_GENERIC_FFT | HF_FOCK_TILE_PLAN)) && fast_length(nk1) &&
+      fast_length(nk2)) {
     plan_rows(nb, sp);
     return HF_OK;
   }
@@ -482,6 +485,28 @@ static int launch_fock(FockParams& p, cudaStream_t stream, bool need_consts) {
   return HF_OK;
 }
 
+// ------------------------------------------------------------ autotuner -----
+// Engine flags chosen by hf_fock_autotune per (device, dtype, flags, nk1, nk2, nb).
+constexpr unsigned kEngineFlags = HF_FOCK_TILE_PLAN | HF_FOCK_GENERIC_FFT;
+using TuneKey = std::tuple<int, int, unsigned, int, int, int>;
+static std::mutex g_tune_mu;
+static std::map<TuneKey, unsigned> g_tune;
+
+static TuneKey tune_key(int dtype, unsigned flags, int nk1, int nk2, int nb) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  return TuneKey(dev, dtype, flags & ~kEngineFlags, nk1, nk2, nb);
+}
+
+// flags with the stored engine choice applied (unless the caller set an engine flag)
+static unsigned tuned_flags(int dtype, unsigned flags, int nk1, int nk2, int nb) {
+  if (flags & kEngineFlags) return flags;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  if (g_tune.empty()) return flags;
+  auto it = g_tune.find(tune_key(dtype, flags, nk1, nk2, nb));
+  return it == g_tune.end() ? flags : (flags | it->second);
+}
+
 }  // namespace hf
 
 using namespace hf;
@@ -490,9 +515,16 @@ extern "C" int hf_fock_workspace_size(int dtype, unsigned flags, int nk1, int nk
   if (!bytes) return fail(HF_ERR_INVALID, "bytes is NULL");
   int st = validate(dtype, flags, nk1, nk2, nb);
   if (st) return st;
-  SlotPlan sp;
-  if ((st = get_plan(dtype, flags, nk1, nk2, nb, sp))) return st;
-  *bytes = ws_layout(sp, nk1, nk2, nb, fft_elem(dtype, flags), (flags & HF_FOCK_EXCHANGE) != 0).total;
+  // every schedule the autotuner may pick (they differ only in the slot plan)
+  size_t most = 0;
+  const unsigned cands[3] = {0u, HF_FOCK_TILE_PLAN, HF_FOCK_GENERIC_FFT};
+  for (unsigned e : cands) {
+    if ((flags & kEngineFlags) && e != 0) continue;
+    SlotPlan sp;
+    if ((st = get_plan(dtype, flags | e, nk1, nk2, nb, sp))) return st;
+    most = std::max(most, ws_layout(sp, nk1, nk2, nb, fft_elem(dtype, flags), (flags & HF_FOCK_EXCHANGE) != 0).total);
+  }
+  *bytes = most;
   return HF_OK;
 }
 
@@ -514,7 +546,8 @@ extern "C" int hf_fock_build(void* stream, int dtype, unsigned flags, int nk1, i
                                  nullptr);
 }
 
-int hf::fock_build_internal(void* stream, int dtype, unsigned flags, int nk1, int nk2, int nb, const void* P,
+// The build with exactly these flags (no stored autotuner choice applied).
+static int fock_build_exact(void* stream, int dtype, unsigned flags, int nk1, int nk2, int nb, const void* P,
                             const void* h, const void* VR, const void* refP, const void* HH, const void* w2d,
                             int n_contact, const void* contact_g, const void* contact_Oi,
                             const void* contact_Oj, void* Sigma, void* H, void* F, void* workspace,
@@ -567,4 +600,82 @@ int hf::fock_build_internal(void* stream, int dtype, unsigned flags, int nk1, in
   if (dtype == HF_C64) return launch_fock<float, float>(p, s, need_consts);
   if (flags & HF_FOCK_FFT_FP32) return launch_fock<double, float>(p, s, need_consts);
   return launch_fock<double, double>(p, s, need_consts);
+}
+
+int hf::fock_build_internal(void* stream, int dtype, unsigned flags, int nk1, int nk2, int nb, const void* P,
+                            const void* h, const void* VR, const void* refP, const void* HH, const void* w2d,
+                            int n_contact, const void* contact_g, const void* contact_Oi,
+                            const void* contact_Oj, void* Sigma, void* H, void* F, void* workspace,
+                            size_t workspace_bytes, const int* active) {
+  const int st = validate(dtype, flags, nk1, nk2, nb);
+  if (st) return st;
+  return fock_build_exact(stream, dtype, tuned_flags(dtype, flags, nk1, nk2, nb), nk1, nk2, nb, P, h, VR, refP, HH,
+                          w2d, n_contact, contact_g, contact_Oi, contact_Oj, Sigma, H, F, workspace, workspace_bytes,
+                          active);
+}
+
+extern "C" int hf_fock_autotune(void* stream, int dtype, unsigned flags, int nk1, int nk2, int nb, const void* P,
+                                const void* h, const void* VR, const void* refP, const void* HH, const void* w2d,
+                                int n_contact, const void* contact_g, const void* contact_Oi,
+                                const void* contact_Oj, void* Sigma, void* H, void* F, void* workspace,
+                                size_t workspace_bytes, int reps, unsigned* chosen, float* us) {
+  using namespace hf;
+  int st = validate(dtype, flags, nk1, nk2, nb);
+  if (st) return st;
+  if (reps < 1) return fail(HF_ERR_INVALID, "reps must be >= 1");
+  if (flags & kEngineFlags) return fail(HF_ERR_INVALID, "hf_fock_autotune chooses the engine flags itself");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const unsigned cands[3] = {0u, HF_FOCK_TILE_PLAN, HF_FOCK_GENERIC_FFT};
+  // the tile candidate only differs from the default where the rows plan applies
+  SlotPlan sp0;
+  if ((st = get_plan(dtype, flags, nk1, nk2, nb, sp0))) return st;
+  float times[3] = {-1.f, -1.f, -1.f};
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  HF_CUDA(cudaEventCreate(&e0));
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return fail(HF_ERR_CUDA, "cudaEventCreate failed");
+  }
+  int best = -1;
+  for (int c = 0; c < 3 && st == HF_OK; ++c) {
+    if (c == 1 && !sp0.rows) continue;
+    const unsigned f = flags | cands[c];
+    auto run = [&] {
+      return fock_build_exact(stream, dtype, f, nk1, nk2, nb, P, h, VR, refP, HH, w2d, n_contact, contact_g,
+                              contact_Oi, contact_Oj, Sigma, H, F, workspace, workspace_bytes, nullptr);
+    };
+    if ((st = run()) != HF_OK) break;
+    if (cudaEventRecord(e0, s) != cudaSuccess) { st = fail(HF_ERR_CUDA, "cudaEventRecord failed"); break; }
+    for (int r = 0; r < reps && st == HF_OK; ++r) st = run();
+    if (st != HF_OK) break;
+    if (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess) {
+      st = fail(HF_ERR_CUDA, "timing the autotuner candidates failed");
+      break;
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    times[c] = 1000.f * ms / (float)reps;
+    if (best < 0 || times[c] < times[best]) best = c;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st != HF_OK) return st;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[tune_key(dtype, flags, nk1, nk2, nb)] = cands[best];
+  }
+  // the outputs hold the winner's result
+  st = fock_build_exact(stream, dtype, flags | cands[best], nk1, nk2, nb, P, h, VR, refP, HH, w2d, n_contact,
+                        contact_g, contact_Oi, contact_Oj, Sigma, H, F, workspace, workspace_bytes, nullptr);
+  if (st != HF_OK) return st;
+  if (chosen) *chosen = cands[best];
+  if (us)
+    for (int c = 0; c < 3; ++c) us[c] = times[c];
+  return HF_OK;
+}
+
+extern "C" int hf_fock_autotune_reset(void) {
+  std::lock_guard<std::mutex> lk(hf::g_tune_mu);
+  hf::g_tune.clear();
+  return HF_OK;
 }

@@ -13,7 +13,12 @@ Differences in form, not in value:
 * ``fft_precision="fp32"`` (extension) runs the exchange FFT of complex128
   inputs in FP32; everything else stays FP64.
 * ``engine="generic"`` (extension, for testing) forces the shared-memory
-  Stockham engine instead of the register FFT of the specialised mesh lengths.
+  Stockham engine instead of the register FFT of the specialised mesh lengths;
+  ``engine="tile"`` forces the 2x2-tile slot groups in the register engine.
+* ``autotune=True`` (extension) times the schedules that apply to this shape
+  (``hf_fock_autotune``), keeps the fastest for every later build of the same
+  shape and flags (solver drivers included) and records the timings in
+  ``last_autotune``.
 """
 
 from __future__ import annotations
@@ -37,6 +42,15 @@ def _as_dev(x, device=None, dtype=None):
     return t.contiguous()
 
 
+# timings of the last build_fock(autotune=True): shape, flags, chosen schedule, us per candidate
+last_autotune: dict = {}
+
+
+def autotune_reset() -> None:
+    """Forgets every schedule stored by build_fock(autotune=True)."""
+    _lib.check(_lib.lib().hf_fock_autotune_reset())
+
+
 def _herm(X: torch.Tensor) -> torch.Tensor:
     return 0.5 * (X + X.transpose(-1, -2).conj())
 
@@ -49,7 +63,8 @@ def build_fock(P, *, h, VR, refP, HH, w2d, include_exchange: bool, include_hartr
                exchange_hermitian_channel_packing: bool, contact_g=None, contact_Oi=None,
                contact_Oj=None, exchange_block_specs=None, exchange_check_offdiag=None,
                exchange_offdiag_atol: float = 1e-12, exchange_offdiag_rtol: float = 0.0,
-               project_fn=None, fft_precision=None, engine=None, hermitian_density: bool = False, out=None):
+               project_fn=None, fft_precision=None, engine=None, hermitian_density: bool = False, out=None,
+               autotune: bool = False, autotune_reps: int = 5):
     """Returns (Sigma, H, F) with F = herm(h + Sigma[P - refP] + H[P - refP]) (fock.py:18-97).
 
     Extensions (keyword-only, defaults keep the reference behaviour): ``fft_precision="fp32"``
@@ -109,6 +124,8 @@ def build_fock(P, *, h, VR, refP, HH, w2d, include_exchange: bool, include_hartr
         flags |= _lib.FOCK_HAS_REFP
     if engine is not None and str(engine).lower() == "generic":
         flags |= _lib.FOCK_GENERIC_FFT
+    elif engine is not None and str(engine).lower() == "tile":
+        flags |= _lib.FOCK_TILE_PLAN
     if fft_precision is not None and str(fft_precision).lower() in ("fp32", "float32", "single"):
         if cdt == torch.complex128:
             flags |= _lib.FOCK_FFT_FP32
@@ -132,10 +149,20 @@ def build_fock(P, *, h, VR, refP, HH, w2d, include_exchange: bool, include_hartr
     need = _lib.C.c_size_t(0)
     _lib.check(_lib.lib().hf_fock_workspace_size(dt, flags, nk1, nk2, nb, _lib.C.byref(need)))
     ws = _lib.workspace(need.value, dev, "fock")
-    _lib.check(_lib.lib().hf_fock_build(
-        _lib.stream_ptr(dev), dt, flags, nk1, nk2, nb, P.data_ptr(), h.data_ptr(), _lib.ptr(VRt),
-        _lib.ptr(refPt), _lib.ptr(HHt), _lib.ptr(w2dt), n_contact, _lib.ptr(cg), _lib.ptr(cOi),
-        _lib.ptr(cOj), Sigma.data_ptr(), H.data_ptr(), F.data_ptr(), ws.data_ptr(), ws.numel()))
+    args = (_lib.stream_ptr(dev), dt, flags, nk1, nk2, nb, P.data_ptr(), h.data_ptr(), _lib.ptr(VRt),
+            _lib.ptr(refPt), _lib.ptr(HHt), _lib.ptr(w2dt), n_contact, _lib.ptr(cg), _lib.ptr(cOi),
+            _lib.ptr(cOj), Sigma.data_ptr(), H.data_ptr(), F.data_ptr(), ws.data_ptr(), ws.numel())
+    if autotune:
+        chosen = _lib.C.c_uint(0)
+        us = (_lib.C.c_float * 3)()
+        _lib.check(_lib.lib().hf_fock_autotune(*args, int(autotune_reps), _lib.C.byref(chosen), us))
+        names = ("default", "tile", "generic")
+        pick = {0: "default", _lib.FOCK_TILE_PLAN: "tile", _lib.FOCK_GENERIC_FFT: "generic"}[chosen.value]
+        last_autotune.clear()
+        last_autotune.update(shape=(nk1, nk2, nb), flags=flags, chosen=pick,
+                             us={n: float(v) for n, v in zip(names, us) if v >= 0})
+    else:
+        _lib.check(_lib.lib().hf_fock_build(*args))
     if project_fn is not None:
         F = _herm(torch.as_tensor(project_fn(F)).to(cdt))
     return Sigma, H, F

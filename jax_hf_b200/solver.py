@@ -142,6 +142,28 @@ class KernelC128:
                           self.w2d.data_ptr(), int(self.cg.shape[0]) if self.has_contact else 0,
                           self.cg.data_ptr(), self.cOi.data_ptr(), self.cOj.data_ptr(), None, None)
 
+    def autotune(self, P, fp32: bool = False, reps: int = 5) -> int:
+        """Runs hf_fock_autotune for this kernel's Fock flags (the ones the CG driver uses) on P
+        (nk1, nk2, nb, nb) complex128; returns the chosen engine flags."""
+        k = self.kernel
+        nk1, nk2, nb = k.shape
+        dev = self.h.device
+        P = torch.as_tensor(P).to(dev, torch.complex128).contiguous()
+        flags = self.flags() | (_lib.FOCK_FFT_FP32 if fp32 else 0)
+        S, F = torch.empty_like(P), torch.empty_like(P)
+        H = torch.empty((nb, nb), dtype=torch.complex128, device=dev)
+        need = C.c_size_t(0)
+        _lib.check(_lib.lib().hf_fock_workspace_size(_lib.HF_C128, flags, nk1, nk2, nb, C.byref(need)))
+        ws = torch.empty(max(int(need.value), 256), dtype=torch.uint8, device=dev)
+        chosen = C.c_uint(0)
+        _lib.check(_lib.lib().hf_fock_autotune(
+            _lib.stream_ptr(dev), _lib.HF_C128, flags, nk1, nk2, nb, P.data_ptr(), self.h.data_ptr(),
+            self.VR.data_ptr(), _lib.ptr(self.refP), self.HH.data_ptr(), self.w2d.data_ptr(),
+            int(self.cg.shape[0]) if self.has_contact else 0, self.cg.data_ptr(), self.cOi.data_ptr(),
+            self.cOj.data_ptr(), S.data_ptr(), H.data_ptr(), F.data_ptr(), ws.data_ptr(), ws.numel(), int(reps),
+            C.byref(chosen), None))
+        return int(chosen.value)
+
     def fock_kwargs(self):
         k = self.kernel
         return dict(h=self.h, VR=self.VR, refP=k.refP if self.refP is None else self.refP, HH=self.HH, w2d=self.w2d,
@@ -263,7 +285,7 @@ class _CgBatchItem(C.Structure):
 
 
 def solve_batch(kernels, P0s, n_electrons, *, config: SolverConfig | None = None, lanes: int = 8,
-                return_times: bool = False):
+                return_times: bool = False, autotune: bool = False):
     """Many independent CG solves in one native call (density scans).
 
     ``kernels``, ``P0s`` and ``n_electrons`` are equal-length sequences; each
@@ -272,6 +294,9 @@ def solve_batch(kernels, P0s, n_electrons, *, config: SolverConfig | None = None
     time, each on its own stream with CUDA-graph iterations, longest first.
     Returns the list of ``SolveResult`` (and, with ``return_times``, each
     solve's device time in ms from its start to its final scalars).
+    ``autotune=True`` first runs the Fock-schedule autotuner (``hf_fock_autotune``) once for
+    every distinct (mesh, nb, Fock flags) of the scan, on that solve's P0; the stored choices
+    then apply to every build of the batch.
     """
     cfg = config or SolverConfig()
     if str(cfg.optimizer).lower() != "cg":
@@ -287,6 +312,15 @@ def solve_batch(kernels, P0s, n_electrons, *, config: SolverConfig | None = None
                      float(cfg.max_step), int(cfg.cg_restart), float(cfg.bt_shrink), int(cfg.bt_max),
                      int(cfg.mu_maxiter), int(cfg.plateau_window), int(bool(cfg.fp32_exchange)),
                      float(cfg.fp32_switch_rel), int(cfg.chunk), FOCK_CB(), PROJECT_CB(), None)
+    if autotune:
+        seen = set()
+        for kern, P0 in zip(kernels, P0s):
+            kc = KernelC128(kern)
+            for fp32 in ((False, True) if cfg.fp32_exchange else (False,)):
+                key = (tuple(kern.shape), kc.flags(), fp32)
+                if key not in seen:
+                    seen.add(key)
+                    kc.autotune(P0, fp32=fp32)
     items = (_CgBatchItem * n)()
     keep, outs = [], []
     for i, (kern, P0, ne) in enumerate(zip(kernels, P0s, n_electrons)):

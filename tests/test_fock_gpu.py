@@ -293,6 +293,39 @@ def test_fast_engine_matches_generic(cuda, n1, n2, nb, V):
     assert rel(Ff, Fg.cpu().numpy()) < TOL64
     Sm, _, Fm = G.build_fock(Pt, fft_precision="fp32", **kw)
     assert rel(Sm, Sg.cpu().numpy()) < TOL32
+    St, _, Ft = G.build_fock(Pt, engine="tile", **kw)  # 2x2-tile slot groups instead of the rows plan
+    assert rel(St, Sg.cpu().numpy()) < TOL64
+    assert rel(Ft, Fg.cpu().numpy()) < TOL64
+
+
+@pytest.mark.parametrize("n1,n2,nb,V,hartree", [(48, 48, 8, "layer", False), (36, 36, 6, "layer", True),
+                                                (24, 24, 4, "scalar", False), (30, 30, 8, "layer", False)])
+def test_autotune_picks_a_schedule_that_matches(cuda, n1, n2, nb, V, hartree):
+    """hf_fock_autotune: every candidate timed, outputs equal the default build, choice reused."""
+    import jax_hf_b200 as G
+    from jax_hf_b200 import fock as Fk
+    prob, P, rng = _problem(n1, n2, nb, V, 7 + n1 + nb)
+    hk = dict(include_hartree=True, hartree_matrix=0.2 + 0.5 * np.eye(nb),
+              reference_density=0.3 * P) if hartree else {}
+    K = G.HartreeFockKernel(prob.weights, prob.hamiltonian, prob.coulomb_q, prob.T, **hk)
+    a = K.as_args()
+    Pt = torch.as_tensor(P, device="cuda")
+    kw = dict(h=a["h"], VR=a["VR"], refP=a["refP"], HH=a["HH"], w2d=K.w2d, include_exchange=True,
+              include_hartree=hartree, exchange_hermitian_channel_packing=a["exchange_hermitian_channel_packing"])
+    Fk.autotune_reset()
+    S0, H0, F0 = G.build_fock(Pt, **kw)
+    try:
+        S1, H1, F1 = G.build_fock(Pt, autotune=True, autotune_reps=2, **kw)
+        info = dict(Fk.last_autotune)
+        assert info["shape"] == (n1, n2, nb)
+        assert info["chosen"] in info["us"] and all(v > 0 for v in info["us"].values())
+        assert "generic" in info["us"] and "default" in info["us"]
+        assert rel(S1, S0.cpu().numpy()) < TOL64 and rel(F1, F0.cpu().numpy()) < TOL64
+        assert rel(H1, H0.cpu().numpy()) < TOL64
+        S2, _, F2 = G.build_fock(Pt, **kw)  # the stored choice
+        assert rel(S2, S0.cpu().numpy()) < TOL64 and rel(F2, F0.cpu().numpy()) < TOL64
+    finally:
+        Fk.autotune_reset()
 
 
 SYM_CASES = [

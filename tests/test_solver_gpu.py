@@ -169,6 +169,27 @@ def test_cg_batch_matches_oracle(cuda):
         assert np.abs(r.density.cpu().numpy() - ro["density"]).max() < 1e-6
 
 
+def test_cg_batch_autotuned_matches_oracle(cuda):
+    """solve_batch(autotune=True): schedules tuned per scan shape, results still the oracle's."""
+    import jax_hf_b200 as G
+    from jax_hf_b200 import fock as Fk
+    from jax_hf_b200.solver import SolverConfig, solve_batch
+    probs = _scan_problems()[:3]
+    cfg = dict(max_iter=150, tol_E=1e-10)
+    Ks = [G.HartreeFockKernel(**p.kernel_kwargs()) for p in probs]
+    P0s = [np.zeros((p.nk, p.nk, p.nb, p.nb), complex) for p in probs]
+    Fk.autotune_reset()
+    try:
+        res = solve_batch(Ks, P0s, [p.n_electrons for p in probs], config=SolverConfig(**cfg), lanes=2,
+                          autotune=True)
+    finally:
+        Fk.autotune_reset()
+    for p, P0, r in zip(probs, P0s, res):
+        ro = O.solve(O.Kernel(**p.kernel_kwargs()), P0, p.n_electrons, config=O.SolverConfig(**cfg))
+        assert abs(float(r.energy) - ro["energy"]) <= 1e-9 * max(1.0, abs(ro["energy"]))
+        assert np.abs(r.density.cpu().numpy() - ro["density"]).max() < 1e-6
+
+
 def test_cg_batch_rejects_hooks(cuda):
     import jax_hf_b200 as G
     from jax_hf_b200.solver import SolverConfig, solve_batch
