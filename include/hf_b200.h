@@ -124,6 +124,19 @@ int hf_fock_autotune(void* stream, int dtype, unsigned flags, int nk1, int nk2, 
 /* Forgets every stored autotuner choice. */
 int hf_fock_autotune_reset(void);
 
+/* Periodic linear resampling of the two leading axes of an (n1, n2, ...)
+ * array on a centered k-grid (k = 0 at index n / 2) to (m1, m2, ...):
+ * utils.py:477-535 (resample_kgrid, method "linear"), axis 0 then axis 1,
+ * positions and weights in the array's real precision.  dtype HF_C128 for
+ * float64 / complex128 data, HF_C64 for float32 / complex64; ncomp = real
+ * components per k-point (2 x elements for complex data).  x and y must not
+ * alias. */
+int hf_resample_kgrid(void* stream, int dtype, int n1, int n2, int m1, int m2, long long ncomp, const void* x,
+                      void* y);
+/* The continuation driver's density seed (continuation.py:47-50):
+ * out = (Q + Q^H) / 2 with Q = resample_kgrid(P), P (n1, n2, nb, nb) complex. */
+int hf_resample_density(void* stream, int dtype, int n1, int n2, int m1, int m2, int nb, const void* P, void* out);
+
 /* ---- Objective reductions (compensated, FP64 accumulation) -----------------
  * hf_energy replaces fock.hf_energy (fock.py:100-111):
  *   E = sum_k w_k Re Tr[(h + (Sigma + H)/2) P]

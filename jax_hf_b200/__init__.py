@@ -8,7 +8,7 @@ call them, running hand-written CUDA kernels through the C ABI in
 
 from .problem import HartreeFockKernel  # noqa: F401
 from .fock import build_fock, hf_energy, free_energy, occupation_entropy  # noqa: F401
-from .utils import find_chemical_potential, fermidirac, validate_electron_count  # noqa: F401
+from .utils import find_chemical_potential, fermidirac, validate_electron_count, resample_kgrid  # noqa: F401
 from . import linalg  # noqa: F401
 
 __all__ = [
@@ -20,5 +20,6 @@ __all__ = [
     "find_chemical_potential",
     "fermidirac",
     "validate_electron_count",
+    "resample_kgrid",
     "linalg",
 ]

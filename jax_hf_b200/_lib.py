@@ -46,6 +46,8 @@ _SIGS = {
     "hf_fock_autotune": ([vp, i32, u32, i32, i32, i32, vp, vp, vp, vp, vp, vp, i32, vp, vp, vp,
                           vp, vp, vp, vp, sz, i32, C.POINTER(C.c_uint), C.POINTER(C.c_float)], i32),
     "hf_fock_autotune_reset": ([], i32),
+    "hf_resample_kgrid": ([vp, i32, i32, i32, i32, i32, C.c_longlong, vp, vp], i32),
+    "hf_resample_density": ([vp, i32, i32, i32, i32, i32, i32, vp, vp], i32),
     "hf_fock_build_static_scratch": ([vp, i32, u32, i32, i32, i32, vp, vp, vp, vp, vp, vp, i32, vp, vp, vp,
                                       vp, vp, vp], i32),
     "hf_reduce_workspace_size": ([i32, i32, i32, psz], i32),

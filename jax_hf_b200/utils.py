@@ -2,7 +2,8 @@
 
 ``find_chemical_potential`` runs the cluster-wide mu root find on the GPU
 (``hf_find_mu``); ``validate_electron_count`` is the reference's host check
-(utils.py:21-43) with the same ValueError text.
+(utils.py:21-43) with the same ValueError text; ``resample_kgrid`` (utils.py:477-535)
+resamples a centered periodic k-grid array on the GPU (``hf_resample_kgrid``).
 """
 
 from __future__ import annotations
@@ -79,3 +80,36 @@ def solve_mu(eps, w_norm, n_target_norm: float, mu0, T: float, maxiter: int = 25
                                      w.data_ptr(), float(n_target_norm), float(T), int(maxiter), m0.data_ptr(),
                                      mu.data_ptr()))
     return mu
+
+
+def resample_kgrid(values, nk: int, *, method: str = "linear") -> torch.Tensor:
+    """Resamples a centered, periodic (nk1, nk2, ...) k-grid array to (nk, nk, ...) (utils.py:512-535).
+
+    Periodic linear interpolation along axis 0 and then axis 1 on the centered grid
+    (k = 0 at index n // 2), on the GPU (``hf_resample_kgrid``); float32/64 and
+    complex64/128 arrays.  Returns the input unchanged when it already is nk x nk.
+    """
+    nk = int(nk)
+    x = values if isinstance(values, torch.Tensor) else torch.as_tensor(np.asarray(values))
+    if x.dim() < 2:
+        raise ValueError("resample_kgrid expects an array with at least 2 dimensions (nk,nk,...).")
+    if x.shape[0] == nk and x.shape[1] == nk:
+        return x
+    if str(method).lower() != "linear":
+        raise ValueError(f"Unsupported resample method {method!r}. Only 'linear' is supported.")
+    if nk <= 0:
+        raise ValueError("n_new must be a positive integer.")
+    if x.dtype not in (torch.float64, torch.float32, torch.complex128, torch.complex64):
+        raise TypeError(f"resample_kgrid: unsupported dtype {x.dtype}")
+    if x.device.type != "cuda":
+        x = x.to(torch.device("cuda", torch.cuda.current_device()))
+    _lib.require_cuda(x)
+    x = x.contiguous()
+    inner = 1
+    for d in x.shape[2:]:
+        inner *= int(d)
+    ncomp = inner * (2 if x.is_complex() else 1)
+    y = torch.empty((nk, nk) + tuple(x.shape[2:]), dtype=x.dtype, device=x.device)
+    _lib.check(_lib.lib().hf_resample_kgrid(_lib.stream_ptr(x.device), _lib.dtype_code(x), int(x.shape[0]),
+                                            int(x.shape[1]), nk, nk, ncomp, x.data_ptr(), y.data_ptr()))
+    return y

@@ -1089,3 +1089,45 @@ def fourier_coefficient_gradient(P, w2d, R):
     K1, K2 = np.meshgrid(k1, k2, indexing="ij")
     w = np.asarray(w2d, np.float64)
     return np.stack([np.einsum("ij,ijab->ab", w * np.exp(-1j * (K1 * Rx + K2 * Ry)), P) for (Rx, Ry) in R])
+
+
+# ---------------------------------------------------------------- continuation ----
+def _resample_axis_periodic_linear(x, n_new, axis):
+    """utils.py:477-509: periodic linear interpolation along one axis of a centered grid
+    (k = 0 at index n // 2); positions and weights in the array's real precision."""
+    x = np.asarray(x)
+    n_old, n_new = int(x.shape[axis]), int(n_new)
+    if n_new <= 0:
+        raise ValueError("n_new must be a positive integer.")
+    if n_old == n_new:
+        return x
+    rd = x.real.dtype
+    j = np.arange(n_new, dtype=rd)
+    u = (j - rd.type(n_new // 2)) * (rd.type(n_old) / rd.type(n_new)) + rd.type(n_old // 2)
+    fl = np.floor(u)
+    i0 = np.mod(fl.astype(np.int64), n_old)
+    i1 = np.mod(i0 + 1, n_old)
+    shape = [1] * x.ndim
+    shape[axis] = n_new
+    frac = (u - fl).reshape(shape).astype(rd)
+    x0, x1 = np.take(x, i0, axis=axis), np.take(x, i1, axis=axis)
+    return ((rd.type(1) - frac) * x0 + frac * x1).astype(x.dtype)
+
+
+def resample_kgrid(values, nk, *, method="linear"):
+    """utils.py:512-535: resample the two leading (centered, periodic) k axes to nk x nk."""
+    nk = int(nk)
+    x = np.asarray(values)
+    if x.ndim < 2:
+        raise ValueError("resample_kgrid expects an array with at least 2 dimensions (nk,nk,...).")
+    if x.shape[0] == nk and x.shape[1] == nk:
+        return x
+    if str(method).lower() != "linear":
+        raise ValueError(f"Unsupported resample method {method!r}. Only 'linear' is supported.")
+    return _resample_axis_periodic_linear(_resample_axis_periodic_linear(x, nk, 0), nk, 1)
+
+
+def resample_density(P, nk):
+    """continuation.py:47-50: resampled density, hermitised."""
+    Q = resample_kgrid(P, nk)
+    return 0.5 * (Q + np.conj(np.swapaxes(Q, -1, -2)))
