@@ -137,6 +137,29 @@ int hf_resample_kgrid(void* stream, int dtype, int n1, int n2, int m1, int m2, l
  * out = (Q + Q^H) / 2 with Q = resample_kgrid(P), P (n1, n2, nb, nb) complex. */
 int hf_resample_density(void* stream, int dtype, int n1, int n2, int m1, int m2, int nb, const void* P, void* out);
 
+/* Symmetry averaging of (nk1, nk2, nb, nb) matrices (symmetry.py:22-150, the
+ * building blocks of make_project_fn; nb <= 32, dtype HF_C128 or HF_C64).
+ * k-point maps: HF_K_FLIP (i -> n - 1 - i, jnp.flip), HF_K_MOD (i -> -i mod n)
+ * on the axes whose bit is set in flip_axes (bit 0: axis 0, bit 1: axis 1), or
+ * HF_K_INDEX_MAP (k -> (idx_i[k], idx_j[k]) from per-element int32 tables).
+ * Index-map entries must lie in [0, nk1) x [0, nk2); an entry outside is
+ * read as the identity map (no out-of-bounds access).  A and out must not
+ * alias. */
+#define HF_K_FLIP 0
+#define HF_K_MOD 1
+#define HF_K_INDEX_MAP 2
+/* out(k) = (sum_{g<n_same} G_same[g] A(k) G_same[g]^H
+ *          + sum_{g<n_mapped} G_mapped[g] A(map_g(k)) G_mapped[g]^H) / (n_same + n_mapped);
+ * index maps idx_i, idx_j: (n_mapped, nk1, nk2).  mask (nk1, nk2) bytes or NULL:
+ * where 0, out(k) = A(k) (spatial_k_orbit_mask). */
+int hf_sym_group_average(void* stream, int dtype, int nk1, int nk2, int nb, const void* A, void* out, int n_same,
+                         const void* G_same, int n_mapped, const void* G_mapped, int k_mode, int flip_axes,
+                         const int* idx_i, const int* idx_j, const unsigned char* mask);
+/* out(k) = (A(k) + U conj(A(-k)) U^H) / 2 with -k from the k-map (index map
+ * (nk1, nk2) tables); with HF_K_INDEX_MAP, out(k) = A(k) where valid[k] == 0. */
+int hf_sym_time_reversal(void* stream, int dtype, int nk1, int nk2, int nb, const void* A, void* out, const void* U,
+                         int k_mode, int flip_axes, const int* idx_i, const int* idx_j, const unsigned char* valid);
+
 /* ---- Objective reductions (compensated, FP64 accumulation) -----------------
  * hf_energy replaces fock.hf_energy (fock.py:100-111):
  *   E = sum_k w_k Re Tr[(h + (Sigma + H)/2) P]

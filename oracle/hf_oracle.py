@@ -1131,3 +1131,86 @@ def resample_density(P, nk):
     """continuation.py:47-50: resampled density, hermitised."""
     Q = resample_kgrid(P, nk)
     return 0.5 * (Q + np.conj(np.swapaxes(Q, -1, -2)))
+
+
+# ------------------------------------------------------------------ symmetry ----
+def _flip_k(A, k_convention, flip_axes=(0, 1)):
+    """symmetry.py:22-44."""
+    if k_convention == "flip":
+        return np.flip(A, axis=tuple(flip_axes))
+    if k_convention == "mod":
+        n1, n2 = A.shape[0], A.shape[1]
+        i = (-np.arange(n1)) % n1 if 0 in flip_axes else np.arange(n1)
+        j = (-np.arange(n2)) % n2 if 1 in flip_axes else np.arange(n2)
+        return A[i[:, None], j[None, :], ...]
+    raise ValueError(f"k_convention must be 'mod' or 'flip', got {k_convention!r}")
+
+
+def _sum_conj(A, G):
+    """symmetry.py:47-56: sum_i g_i A g_i^H."""
+    acc = np.zeros_like(A)
+    for g in G:
+        acc = acc + (g @ A) @ np.conj(g.T)
+    return acc
+
+
+def make_project_fn(*, unitary_group=None, spatial_group=None, spatial_k_convention="mod",
+                    spatial_k_flip_axes=(0, 1), spatial_k_index_maps=None, spatial_k_orbit_mask=None,
+                    time_reversal_U=None, time_reversal_k_convention="mod", time_reversal_k_flip_axes=(0, 1),
+                    time_reversal_k_index_map=None):
+    """symmetry.py:153-281, NumPy restatement (same composition order and checks)."""
+    G = None if unitary_group is None else np.asarray(unitary_group)
+    S = None if spatial_group is None else np.asarray(spatial_group)
+    U = None if time_reversal_U is None else np.asarray(time_reversal_U)
+    if G is None and S is None and spatial_k_index_maps is None and U is None:
+        return lambda A: A
+    if spatial_k_index_maps is not None:
+        si, sj = (np.asarray(m, dtype=np.int64) for m in spatial_k_index_maps)
+        if si.shape != sj.shape:
+            raise ValueError("spatial_k_index_maps[0] and [1] must have the same shape; "
+                             f"got {si.shape} vs {sj.shape}.")
+        if S is None:
+            raise ValueError("spatial_k_index_maps requires spatial_group (the orbital unitaries to average over).")
+        if S.shape[0] != si.shape[0]:
+            raise ValueError("spatial_group and spatial_k_index_maps must have matching "
+                             f"leading dim; got {S.shape[0]} and {si.shape[0]}.")
+    else:
+        si = sj = None
+    omask = None if spatial_k_orbit_mask is None else np.asarray(spatial_k_orbit_mask, dtype=bool)
+    if time_reversal_k_index_map is not None:
+        if U is None:
+            raise ValueError("time_reversal_k_index_map requires time_reversal_U.")
+        ti, tj = (np.asarray(m, dtype=np.int64) for m in time_reversal_k_index_map[:2])
+        tv = np.asarray(time_reversal_k_index_map[2], dtype=bool)
+    else:
+        ti = tj = tv = None
+    sconv, saxes = str(spatial_k_convention), tuple(spatial_k_flip_axes)
+    tconv, taxes = str(time_reversal_k_convention), tuple(time_reversal_k_flip_axes)
+
+    def project(A):
+        out = np.asarray(A)
+        if si is not None:
+            acc = np.zeros_like(out)
+            for g in range(S.shape[0]):
+                acc = acc + (S[g] @ out[si[g], sj[g]]) @ np.conj(S[g].T)
+            avg = acc / S.shape[0]
+            out = np.where(omask[..., None, None], avg, out) if omask is not None else avg
+            if G is not None:
+                out = _sum_conj(out, G) / G.shape[0]
+        elif G is not None and S is not None:
+            out = (_sum_conj(out, G) + _sum_conj(_flip_k(out, sconv, saxes), S)) / (G.shape[0] + S.shape[0])
+        elif G is not None:
+            out = _sum_conj(out, G) / G.shape[0]
+        elif S is not None:
+            eye = np.eye(S.shape[-1], dtype=S.dtype)[None]
+            out = (_sum_conj(out, eye) + _sum_conj(_flip_k(out, sconv, saxes), S)) / (1 + S.shape[0])
+        if U is not None:
+            UH = np.conj(U.T)
+            if ti is not None:
+                Atr = U @ np.conj(out[ti, tj]) @ UH
+                out = np.where(tv[..., None, None], 0.5 * (out + Atr), out)
+            else:
+                out = 0.5 * (out + U @ np.conj(_flip_k(out, tconv, taxes)) @ UH)
+        return out
+
+    return project

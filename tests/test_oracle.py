@@ -240,3 +240,23 @@ def test_newton_hvp_matches_finite_difference():
                      np.abs(proj((gpe - gp0) / e) - Hp).max() / np.abs(Hp).max()))
     assert errs[1][0] < 1e-4 and errs[1][1] < 1e-4
     assert errs[1][0] < 0.2 * errs[0][0] + 1e-12
+
+
+def test_oracle_symmetry_projector_properties():
+    """Restatement of make_project_fn (symmetry.py:153-281) on the reference's property tests."""
+    rng = np.random.default_rng(4)
+    A = rng.standard_normal((4, 4, 4, 4)) + 1j * rng.standard_normal((4, 4, 4, 4))
+    G = np.stack([np.eye(4), np.diag([1, 1, -1, -1]).astype(complex)])
+    p = O.make_project_fn(unitary_group=G)
+    B = p(A)
+    for g in G:
+        np.testing.assert_allclose(g @ B @ np.conj(g.T), B, atol=1e-14)
+    np.testing.assert_allclose(p(B), B, atol=1e-14)
+    U = np.array([[0, -1j], [1j, 0]])
+    A2 = A[..., :2, :2]
+    for conv in ("flip", "mod"):
+        q = O.make_project_fn(time_reversal_U=U, time_reversal_k_convention=conv)
+        C = q(A2)
+        Cneg = O._flip_k(C, conv)
+        np.testing.assert_allclose(U @ np.conj(Cneg) @ np.conj(U.T), C, atol=1e-14)
+    assert O.make_project_fn()(A) is A
