@@ -160,6 +160,21 @@ int hf_sym_group_average(void* stream, int dtype, int nk1, int nk2, int nb, cons
 int hf_sym_time_reversal(void* stream, int dtype, int nk1, int nk2, int nb, const void* A, void* out, const void* U,
                          int k_mode, int flip_axes, const int* idx_i, const int* idx_j, const unsigned char* valid);
 
+/* Superlattice Fock exchange on the extended momentum grid (superlattice.py:
+ * 167-229, make_superlattice_fock_fn), complex128: rho and sigma are
+ * (nkx, nky, n_G dim_orb, n_G dim_orb); V_lag_fft is (N_ext_x, N_ext_y)
+ * complex128 (the layout's FFT of the lag Coulomb kernel); g_a_off (n_G, 2)
+ * int32 tile offsets; pair_to_delta (n_G, n_G) int32 DG index of each pair;
+ * tile_owner (n_delta, N_ext_x / nkx, N_ext_y / nky) int32: i n_G + j of the
+ * pair (i, j) of that DG whose tile sits there, or -1.  All DG channels are
+ * transformed with the library's exchange build in chunks of up to 1024
+ * channels; workspace from hf_sl_fock_workspace_size. */
+int hf_sl_fock_workspace_size(int nkx, int nky, int n_G, int dim_orb, int N_ext_x, int N_ext_y, int n_delta,
+                              size_t* bytes);
+int hf_sl_fock(void* stream, int nkx, int nky, int n_G, int dim_orb, int N_ext_x, int N_ext_y, int n_delta,
+               const int* tile_owner, const int* g_a_off, const int* pair_to_delta, const void* V_lag_fft,
+               const void* rho, void* sigma, void* workspace, size_t workspace_bytes);
+
 /* ---- Objective reductions (compensated, FP64 accumulation) -----------------
  * hf_energy replaces fock.hf_energy (fock.py:100-111):
  *   E = sum_k w_k Re Tr[(h + (Sigma + H)/2) P]

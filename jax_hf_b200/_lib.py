@@ -50,6 +50,8 @@ _SIGS = {
     "hf_resample_density": ([vp, i32, i32, i32, i32, i32, i32, vp, vp], i32),
     "hf_sym_group_average": ([vp, i32, i32, i32, i32, vp, vp, i32, vp, i32, vp, i32, i32, vp, vp, vp], i32),
     "hf_sym_time_reversal": ([vp, i32, i32, i32, i32, vp, vp, vp, i32, i32, vp, vp, vp], i32),
+    "hf_sl_fock_workspace_size": ([i32, i32, i32, i32, i32, i32, i32, psz], i32),
+    "hf_sl_fock": ([vp, i32, i32, i32, i32, i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, sz], i32),
     "hf_fock_build_static_scratch": ([vp, i32, u32, i32, i32, i32, vp, vp, vp, vp, vp, vp, i32, vp, vp, vp,
                                       vp, vp, vp], i32),
     "hf_reduce_workspace_size": ([i32, i32, i32, psz], i32),

@@ -1214,3 +1214,61 @@ def make_project_fn(*, unitary_group=None, spatial_group=None, spatial_k_convent
         return out
 
     return project
+
+
+# -------------------------------------------------------------- superlattice ----
+def sl_build_extended_layout(g_frac, B, nkx, nky, coulomb_V, w_scalar):
+    """superlattice.py:72-164 restated with explicit loops; returns a dict of the tables."""
+    g = np.asarray(g_frac, dtype=np.int64)
+    nG = g.shape[0]
+    pg = -g
+    gx0, gx1, gy0, gy1 = pg[:, 0].min(), pg[:, 0].max(), pg[:, 1].min(), pg[:, 1].max()
+    Nx, Ny = 2 * nkx * (gx1 - gx0 + 1), 2 * nky * (gy1 - gy0 + 1)
+    off = np.stack([pg[:, 0] - gx0, pg[:, 1] - gy0], axis=1)
+    dset, p2d = {}, np.empty((nG, nG), dtype=np.int64)
+    for i in range(nG):
+        for j in range(nG):
+            key = (int(g[i, 0] - g[j, 0]), int(g[i, 1] - g[j, 1]))
+            if key not in dset:
+                dset[key] = len(dset)
+            p2d[i, j] = dset[key]
+    nd = len(dset)
+    cnt = np.zeros(nd, dtype=np.int64)
+    for i in range(nG):
+        for j in range(nG):
+            cnt[p2d[i, j]] += 1
+    start = np.zeros(nd + 1, dtype=np.int64)
+    start[1:] = np.cumsum(cnt)
+    pi, pj, cur = np.empty(start[-1], np.int64), np.empty(start[-1], np.int64), start.copy()
+    for i in range(nG):
+        for j in range(nG):
+            d = p2d[i, j]
+            pi[cur[d]], pj[cur[d]] = i, j
+            cur[d] += 1
+    ix, iy = np.arange(Nx), np.arange(Ny)
+    fx, fy = np.meshgrid(np.where(ix < Nx // 2, ix, ix - Nx) / float(nkx), np.where(iy < Ny // 2, iy, iy - Ny) / float(nky),
+                         indexing="ij")
+    B = np.asarray(B, dtype=float)
+    q = np.sqrt((B[0, 0] * fx + B[0, 1] * fy) ** 2 + (B[1, 0] * fx + B[1, 1] * fy) ** 2)
+    V = np.fft.fftn(float(w_scalar) * np.asarray(coulomb_V(q), dtype=float), axes=(0, 1))
+    return dict(N_ext_x=Nx, N_ext_y=Ny, g_a_off=off, n_delta=nd, pair_to_delta=p2d, delta_pair_i=pi,
+                delta_pair_j=pj, delta_pair_start=start, V_lag_fft=V)
+
+
+def sl_streaming_fock(rho, L, nG, dorb, nkx, nky):
+    """superlattice.py:202-229: per DG channel scatter, -IFFT2(FFT2 * V_lag_fft), gather."""
+    rr = np.asarray(rho).reshape(nkx, nky, nG, dorb, nG, dorb)
+    sig = np.empty_like(rr)
+    for d in range(L["n_delta"]):
+        buf = np.zeros((L["N_ext_x"], L["N_ext_y"], dorb, dorb), dtype=complex)
+        ks = range(L["delta_pair_start"][d], L["delta_pair_start"][d + 1])
+        for k in ks:
+            i, j = L["delta_pair_i"][k], L["delta_pair_j"][k]
+            ox, oy = nkx * L["g_a_off"][i, 0], nky * L["g_a_off"][i, 1]
+            buf[ox:ox + nkx, oy:oy + nky] = rr[:, :, i, :, j, :]
+        s = -np.fft.ifftn(np.fft.fftn(buf, axes=(0, 1)) * L["V_lag_fft"][:, :, None, None], axes=(0, 1))
+        for k in ks:
+            i, j = L["delta_pair_i"][k], L["delta_pair_j"][k]
+            ox, oy = nkx * L["g_a_off"][i, 0], nky * L["g_a_off"][i, 1]
+            sig[:, :, i, :, j, :] = s[ox:ox + nkx, oy:oy + nky]
+    return sig.reshape(nkx, nky, nG * dorb, nG * dorb)
