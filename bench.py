@@ -273,7 +273,8 @@ def run_solves(dev):
     scfg = SCFConfig(acceleration="diis")
     for _ in range(3):  # first calls load kernels and capture / instantiate graphs
         solve_scf(K0, P00, p0.n_electrons, config=scfg)
-    r0, ms0 = ev_time(lambda: solve_scf(K0, P00, p0.n_electrons, config=scfg), reps=3)
+    runs0 = [ev_time(lambda: solve_scf(K0, P00, p0.n_electrons, config=scfg)) for _ in range(7)]
+    r0, ms0 = runs0[0][0], float(statistics.median(t for _, t in runs0))  # median of 7 single solves
     out["scf_diis_24x24_nb4_fp64"] = {"solves_per_s": round(1e3 / ms0, 2), "ms_per_solve": round(ms0, 2),
                                      "iterations": int(r0.iterations), "converged": bool(r0.converged),
                                      "energy": float(r0.energy)}
@@ -286,7 +287,8 @@ def run_solves(dev):
                       ("mixed", SolverConfig(max_iter=400, tol_E=1e-9, fp32_exchange=True))):
         for _ in range(3):  # first calls load kernels and capture / instantiate graphs
             solve(K2, P02, p2.n_electrons, config=cfg)
-        r, ms = ev_time(lambda: solve(K2, P02, p2.n_electrons, config=cfg), reps=3)
+        runs = [ev_time(lambda: solve(K2, P02, p2.n_electrons, config=cfg)) for _ in range(7)]
+        r, ms = runs[0][0], float(statistics.median(t for _, t in runs))  # median of 7 single solves
         res[name] = (r, ms)
     E64 = float(res["fp64"][0].energy)
     cg2 = {}
