@@ -290,6 +290,17 @@ def run_solves(dev):
         torch.cuda.synchronize()
         return out, e0.elapsed_time(e1) / reps
 
+    def median_run(fn, n):
+        # median time of n calls; only the last result is kept, so the caching allocator can reuse
+        # the previous call's output blocks (holding every result would force fresh device
+        # allocations inside the timed calls)
+        ts, res = [], None
+        for _ in range(n):
+            res = None
+            res, t = ev_time(fn)
+            ts.append(t)
+        return res, float(statistics.median(ts))
+
     out = {}
     # SCF-DIIS 24x24 nb=4
     p0 = S.scf_diis_24()
@@ -298,8 +309,7 @@ def run_solves(dev):
     scfg = SCFConfig(acceleration="diis")
     for _ in range(3):  # first calls load kernels and capture / instantiate graphs
         solve_scf(K0, P00, p0.n_electrons, config=scfg)
-    runs0 = [ev_time(lambda: solve_scf(K0, P00, p0.n_electrons, config=scfg)) for _ in range(7)]
-    r0, ms0 = runs0[0][0], float(statistics.median(t for _, t in runs0))  # median of 7 single solves
+    r0, ms0 = median_run(lambda: solve_scf(K0, P00, p0.n_electrons, config=scfg), 7)
     out["scf_diis_24x24_nb4_fp64"] = {"solves_per_s": round(1e3 / ms0, 2), "ms_per_solve": round(ms0, 2),
                                      "iterations": int(r0.iterations), "converged": bool(r0.converged),
                                      "energy": float(r0.energy)}
@@ -312,8 +322,7 @@ def run_solves(dev):
                       ("mixed", SolverConfig(max_iter=400, tol_E=1e-9, fp32_exchange=True))):
         for _ in range(3):  # first calls load kernels and capture / instantiate graphs
             solve(K2, P02, p2.n_electrons, config=cfg)
-        runs = [ev_time(lambda: solve(K2, P02, p2.n_electrons, config=cfg)) for _ in range(7)]
-        r, ms = runs[0][0], float(statistics.median(t for _, t in runs))  # median of 7 single solves
+        r, ms = median_run(lambda: solve(K2, P02, p2.n_electrons, config=cfg), 7)
         res[name] = (r, ms)
     E64 = float(res["fp64"][0].energy)
     cg2 = {}
@@ -347,7 +356,7 @@ def run_solves(dev):
                                     "p50_ms": round(float(np.percentile(t_one, 50)), 2),
                                     "p99_ms": round(float(np.percentile(t_one, 99)), 2)}}
     for name, cfg in (("fp64_batched", c64), ("mixed_batched", cmx)):
-        (rb, tb), ms = ev_time(lambda: solve_batch(Ks, P0s, nes, config=cfg, lanes=16, return_times=True))
+        (rb, tb), ms = median_run(lambda: solve_batch(Ks, P0s, nes, config=cfg, lanes=16, return_times=True), 3)
         Eb = np.array([float(r.energy) for r in rb])
         rel = np.abs(Eb - E_one) / np.abs(E_one)
         scan[name] = {"solves_per_s": round(len(probs) / (ms / 1e3), 2), "total_ms": round(ms, 2),

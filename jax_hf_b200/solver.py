@@ -185,7 +185,7 @@ def _solve_cg(kernel, P0, n_electrons, cfg: SolverConfig, fock_build_fn=None):
                      float(cfg.fp32_switch_rel), int(cfg.chunk), FOCK_CB(), PROJECT_CB(), None)
     need = C.c_size_t(0)
     _lib.check(L.hf_cg_workspace_size(C.byref(prob), C.byref(conf), C.byref(need)))
-    ws = torch.empty(need.value, dtype=torch.uint8, device=dev)
+    ws = _lib.workspace(need.value, dev, "cg")
     P0t = torch.as_tensor(P0).to(dev, torch.complex128).contiguous() if not (
         isinstance(P0, torch.Tensor) and P0.dtype == torch.complex128 and P0.device == dev) else P0.contiguous()
     Q = torch.empty((nk1, nk2, nb, nb), dtype=torch.complex128, device=dev)
@@ -323,17 +323,37 @@ def solve_batch(kernels, P0s, n_electrons, *, config: SolverConfig | None = None
                     kc.autotune(P0, fp32=fp32)
     items = (_CgBatchItem * n)()
     keep, outs = [], []
+    # All outputs of the batch are views of one allocation (one allocator call per batch instead of
+    # seven per solve); the block lives as long as any returned tensor does.
+    nh = max(cfg.max_iter, 1)
+    shapes = [tuple(k.shape) for k in kernels]
+    al = lambda b: (b + 255) // 256 * 256
+    per = [3 * al(a * b * c * c * 16) + al(a * b * c * 8) + 2 * al(nh * 8) for (a, b, c) in shapes]
+    block = torch.empty(sum(per) + al(n * 64), dtype=torch.uint8, device=dev)
+    cursor = [0]
+
+    def take(count, dtype, shape):
+        o = cursor[0]
+        nbytes = count * torch.empty((), dtype=dtype).element_size()
+        cursor[0] = o + al(nbytes)
+        return block[o:o + nbytes].view(dtype).view(shape)
+
+    scs = take(n * 8, torch.float64, (n, 8))  # every solve's scalars, read back in one copy
+    scs.zero_()
     for i, (kern, P0, ne) in enumerate(zip(kernels, P0s, n_electrons)):
         validate_electron_count(kern.w2d, kern.h.shape[-1], ne, context="n_electrons")
         nk1, nk2, nb = kern.shape
         kc = KernelC128(kern)
         P0t = torch.as_tensor(P0).to(dev, torch.complex128).contiguous()
-        Q = torch.empty((nk1, nk2, nb, nb), dtype=torch.complex128, device=dev)
-        p = torch.empty((nk1, nk2, nb), dtype=torch.float64, device=dev)
-        P, F = torch.empty_like(Q), torch.empty_like(Q)
-        hE = torch.zeros(max(cfg.max_iter, 1), dtype=torch.float64, device=dev)
-        hG = torch.zeros(max(cfg.max_iter, 1), dtype=torch.float64, device=dev)
-        sc = torch.zeros(8, dtype=torch.float64, device=dev)
+        Q = take(nk1 * nk2 * nb * nb, torch.complex128, (nk1, nk2, nb, nb))
+        p = take(nk1 * nk2 * nb, torch.float64, (nk1, nk2, nb))
+        P = take(nk1 * nk2 * nb * nb, torch.complex128, (nk1, nk2, nb, nb))
+        F = take(nk1 * nk2 * nb * nb, torch.complex128, (nk1, nk2, nb, nb))
+        hE = take(nh, torch.float64, (nh,))
+        hG = take(nh, torch.float64, (nh,))
+        hE.zero_()
+        hG.zero_()
+        sc = scs[i]
         items[i] = _CgBatchItem(kc.problem(ne), P0t.data_ptr(), Q.data_ptr(), p.data_ptr(), P.data_ptr(),
                                 F.data_ptr(), hE.data_ptr(), hG.data_ptr(), sc.data_ptr())
         keep += [kc, P0t]
@@ -341,13 +361,14 @@ def solve_batch(kernels, P0s, n_electrons, *, config: SolverConfig | None = None
     per_lane = C.c_size_t(0)
     _lib.check(L.hf_cg_batch_workspace_size(items, n, C.byref(conf), C.byref(per_lane)))
     lanes = max(1, min(int(lanes), n))
-    ws = torch.empty(lanes * per_lane.value, dtype=torch.uint8, device=dev)
+    ws = _lib.workspace(lanes * per_lane.value, dev, "cg_batch")
     times = (C.c_double * n)()
     _lib.check(L.hf_cg_solve_batch(_lib.stream_ptr(dev), items, n, C.byref(conf), lanes, ws.data_ptr(),
                                    per_lane.value, times))
     results = []
-    for kern, Q, p, P, F, hE, hG, sc in outs:
-        s = sc.cpu().numpy()
+    host = scs.cpu().numpy()
+    for i, (kern, Q, p, P, F, hE, hG, sc) in enumerate(outs):
+        s = host[i]
         hist = dict(E=hE[:cfg.max_iter].to(kern.real_dtype), grad_norm=hG[:cfg.max_iter].to(kern.real_dtype),
                     fp32_switch_iter=int(s[5]))
         results.append(SolveResult(Q=Q.to(kern.dtype), p=p.to(kern.real_dtype), mu=sc[0].to(kern.real_dtype),
