@@ -101,9 +101,9 @@ int hf_fock_build_static_scratch(void* stream, int dtype, unsigned flags, int nk
                                  const void* contact_Oi, const void* contact_Oj, void* Sigma, void* H,
                                  void* F);
 
-/* Autotuner for the Fock-build schedule (the north-star's "tile and radix
- * schedules picked by an autotuner"; no counterpart in the reference, whose
- * FFTs are XLA's).  Same arguments as hf_fock_build, plus reps (timed builds
+/* Autotuner for the Fock-build schedule (slot plan and FFT engine per shape;
+ * no counterpart in the reference, whose FFTs are XLA's).  Same arguments as
+ * hf_fock_build, plus reps (timed builds
  * per candidate, >= 1), chosen (out: the engine flags picked) and us (out,
  * may be NULL: mean microseconds per build of each candidate, in the order
  * default schedule / HF_FOCK_TILE_PLAN / HF_FOCK_GENERIC_FFT, -1 for a
