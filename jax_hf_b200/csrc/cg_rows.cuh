@@ -309,6 +309,10 @@ __device__ __forceinline__ double diag_uhfu_col(const double2 (&u)[NB], const do
 }
 
 // -------------------- line-search trials i0 <= i < i1 on the frozen-F free energy
+// The first trial (NT = 1, i0 = 0) also forms, speculatively, what the retraction
+// would write if tau0 is accepted: eps = diag(U^H Ft U) into eps and Q U into Vd
+// (same arithmetic as k_cgr_update); its last CTA sets first_ok when tau0 is
+// accepted, and k_cgr_update then only copies Vd into Q.
 template <int NB, int NT>
 __global__ void __launch_bounds__(32 * kRowWarps) k_cgr_trials(CgArgs a, int i0, int i1, int last_chunk) {
   if (!cg_active(a)) return;
@@ -359,12 +363,30 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_cgr_trials(CgArgs a, int i0,
     for (int it = 0; it < NT; ++it) {
       if (it < nt) {  // warp-uniform
         double2 u[NB];
-        cayley_cols<NB>(d, taus[it], c, on, SC, SX, u);
+        cayley_cols<NB>(d, taus[it], c, on, SC, SX, u);  // ends with a warp barrier: SX is free again
         if (on) {
           const double et = diag_uhfu_col<NB>(u, SFt);
           const double pt = clip(pv - taus[it] * dpv, 1e-8, 1.0 - 1e-8);
           se[it] += wk * pt * et;
           sh[it] += wk * ent_term(pt);
+          if (NT == 1 && i0 == 0) {
+            a.eps[(size_t)k * NB + c] = et;
+#pragma unroll
+            for (int r = 0; r < NB; ++r) SX[r * LP + c] = a.Q[base + (size_t)r * NB];
+          }
+        }
+        if (NT == 1 && i0 == 0) {
+          __syncwarp();
+          if (on) {
+#pragma unroll
+            for (int r = 0; r < NB; ++r) {  // (Q U)[r][c] = sum_j Q[r][j] U[j][c]
+              double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+              for (int j = 0; j < NB; ++j) acc = cfma(SX[r * LP + j], u[j], acc);
+              a.Vd[base + (size_t)r * NB] = acc;
+            }
+          }
+          __syncwarp();  // SX is the Cayley stage of the next k-point group
         }
       }
     }
@@ -386,6 +408,7 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_cgr_trials(CgArgs a, int i0,
         if (om < s->Omega0) {
           s->accepted = 1;
           s->tau_final = taus[it];
+          if (NT == 1 && i0 == 0 && it == 0) s->first_ok = 1;
           break;
         }
       }
@@ -398,6 +421,12 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_cgr_trials(CgArgs a, int i0,
 template <int NB>
 __global__ void __launch_bounds__(32 * kRowWarps) k_cgr_update(CgArgs a) {
   if (!cg_active(a)) return;
+  if (a.sc->first_ok) {  // tau0 accepted: the first trial formed eps and Q U(tau0) already
+    const size_t nq = (size_t)a.nk * NB * NB;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < nq; e += (size_t)gridDim.x * blockDim.x)
+      a.Q[e] = a.Vd[e];
+    return;
+  }
   using RG = RowGroup<NB>;
   constexpr int G = RG::G, KPW = RG::KPW, LP = RG::LP, MAT = RG::MAT;
   __shared__ double2 st[kRowWarps][KPW][2 * MAT + NB];

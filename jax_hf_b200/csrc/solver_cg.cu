@@ -36,7 +36,8 @@ int find_mu_internal(void* stream, int dtype, int method, int nk1, int nk2, int 
                      double* mu_out, const int* active);
 
 struct CgScalars {
-  int k, active, accepted, converged, k_base, pad_;
+  int k, active, accepted, converged, k_base;
+  int first_ok;  // the first line-search trial was accepted: Q U(tau0) and eps are already in Vd / eps
   double mu, E, E_prev, dE, grad_norm;
   double lam, pr_den, beta, tau0, tau_final, Omega0, E_fin;
 };
@@ -44,7 +45,7 @@ struct CgScalars {
 struct CgArgs {
   int nk, nb, max_iter, cg_restart, bt_max, plateau_window;
   double T_r, tol_E, tol_grad, denom_scale, max_step, bt_shrink, n_target_norm;
-  double2 *Q, *P, *F, *Ft, *G0, *G1, *dQ, *Vd, *Fe;
+  double2 *Q, *P, *F, *Ft, *G0, *G1, *dQ, *Vd, *Fe;  // Vd: eigenvectors of i d (warp path), Q U(tau0) (row path)
   double *p, *eps, *epsF, *gp0, *gp1, *dp, *lamd, *w_norm;
   double* hist_E;
   double* hist_G;
@@ -84,6 +85,7 @@ __global__ void k_cg_init(CgArgs a, const double2* __restrict__ P0, const double
     s->k_base = 0;
     s->active = a.max_iter > 0 ? 1 : 0;
     s->accepted = 0;
+    s->first_ok = 0;
     s->converged = 0;
     s->mu = 0.0;
     s->E = 0.0;
@@ -351,6 +353,7 @@ __global__ void __launch_bounds__(256) k_cg_dir_t(CgArgs a) {
       sc->tau0 = fmin(1.0, a.max_step / fmax(dn, 1e-30));
       sc->Omega0 = tot[1] + fmax(a.T_r, 1e-14) * tot[2];
       sc->accepted = 0;
+      sc->first_ok = 0;
       sc->tau_final = sc->tau0;
     }
   }
@@ -475,6 +478,7 @@ __global__ void k_cg_dir(CgArgs a) {
       s->tau0 = fmin(1.0, a.max_step / fmax(dn, 1e-30));
       s->Omega0 = tot[1] + fmax(a.T_r, 1e-14) * tot[2];
       s->accepted = 0;
+      s->first_ok = 0;
       s->tau_final = s->tau0;
     }
   }
@@ -518,6 +522,7 @@ __global__ void k_cg_dir_lu(CgArgs a) {
       s->tau0 = fmin(1.0, a.max_step / fmax(dn, 1e-30));
       s->Omega0 = tot[1] + fmax(a.T_r, 1e-14) * tot[2];
       s->accepted = 0;
+      s->first_ok = 0;
       s->tau_final = s->tau0;
     }
   }
