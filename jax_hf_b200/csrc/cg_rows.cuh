@@ -139,6 +139,7 @@ __device__ __forceinline__ void cayley_cols(const double2 (&d)[NB], double tau, 
 template <int NB>
 __global__ void __launch_bounds__(32 * kRowWarps) k_cgr_density(CgArgs a, int force) {
   if (!force && !cg_active(a)) return;
+  double2* const Qc = q_cur(a);
   using RG = RowGroup<NB>;
   constexpr int G = RG::G, KPW = RG::KPW, LP = RG::LP, MAT = RG::MAT;
   __shared__ double2 st[kRowWarps][KPW][2 * MAT];
@@ -154,7 +155,7 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_cgr_density(CgArgs a, int fo
     const size_t base = (size_t)k * NB * NB + c;
     if (on) {
 #pragma unroll
-      for (int r = 0; r < NB; ++r) SQ[r * LP + c] = a.Q[base + (size_t)r * NB];
+      for (int r = 0; r < NB; ++r) SQ[r * LP + c] = Qc[base + (size_t)r * NB];
       const double pv = sigmoid((mu - a.eps[(size_t)k * NB + c]) / Tr);
       a.p[(size_t)k * NB + c] = pv;
       SPv[c] = pv;
@@ -190,6 +191,7 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_cgr_density(CgArgs a, int fo
 template <int NB>
 __global__ void __launch_bounds__(32 * kRowWarps) k_cgr_grad1(CgArgs a) {
   if (!cg_active(a)) return;
+  double2* const Qc = q_cur(a);
   using RG = RowGroup<NB>;
   constexpr int G = RG::G, KPW = RG::KPW, LP = RG::LP, MAT = RG::MAT;
   __shared__ double2 st[kRowWarps][KPW][2 * MAT];
@@ -215,7 +217,7 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_cgr_grad1(CgArgs a) {
     if (on) {
 #pragma unroll
       for (int r = 0; r < NB; ++r) {
-        q[r] = a.Q[base + (size_t)r * NB];
+        q[r] = Qc[base + (size_t)r * NB];
         SQ[r * LP + c] = q[r];
         SF[r * LP + c] = a.F[base + (size_t)r * NB];
       }
@@ -372,7 +374,7 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_cgr_trials(CgArgs a, int i0,
           if (NT == 1 && i0 == 0) {
             a.eps[(size_t)k * NB + c] = et;
 #pragma unroll
-            for (int r = 0; r < NB; ++r) SX[r * LP + c] = a.Q[base + (size_t)r * NB];
+            for (int r = 0; r < NB; ++r) SX[r * LP + c] = q_cur(a)[base + (size_t)r * NB];
           }
         }
         if (NT == 1 && i0 == 0) {
@@ -383,7 +385,7 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_cgr_trials(CgArgs a, int i0,
               double2 acc = make_double2(0.0, 0.0);
 #pragma unroll
               for (int j = 0; j < NB; ++j) acc = cfma(SX[r * LP + j], u[j], acc);
-              a.Vd[base + (size_t)r * NB] = acc;
+              q_alt(a)[base + (size_t)r * NB] = acc;
             }
           }
           __syncwarp();  // SX is the Cayley stage of the next k-point group
@@ -408,7 +410,10 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_cgr_trials(CgArgs a, int i0,
         if (om < s->Omega0) {
           s->accepted = 1;
           s->tau_final = taus[it];
-          if (NT == 1 && i0 == 0 && it == 0) s->first_ok = 1;
+          if (NT == 1 && i0 == 0 && it == 0) {  // the other buffer holds Q U(tau0): make it current
+            s->first_ok = 1;
+            s->qsel ^= 1;
+          }
           break;
         }
       }
@@ -421,12 +426,8 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_cgr_trials(CgArgs a, int i0,
 template <int NB>
 __global__ void __launch_bounds__(32 * kRowWarps) k_cgr_update(CgArgs a) {
   if (!cg_active(a)) return;
-  if (a.sc->first_ok) {  // tau0 accepted: the first trial formed eps and Q U(tau0) already
-    const size_t nq = (size_t)a.nk * NB * NB;
-    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < nq; e += (size_t)gridDim.x * blockDim.x)
-      a.Q[e] = a.Vd[e];
-    return;
-  }
+  if (a.sc->first_ok) return;  // tau0 accepted: the first trial formed eps and Q U(tau0) already
+  double2* const Qc = q_cur(a);
   using RG = RowGroup<NB>;
   constexpr int G = RG::G, KPW = RG::KPW, LP = RG::LP, MAT = RG::MAT;
   __shared__ double2 st[kRowWarps][KPW][2 * MAT + NB];
@@ -456,7 +457,7 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_cgr_update(CgArgs a) {
     if (on) {
       a.eps[(size_t)k * NB + c] = diag_uhfu_col<NB>(u, SFt);
 #pragma unroll
-      for (int r = 0; r < NB; ++r) SX[r * LP + c] = a.Q[base + (size_t)r * NB];
+      for (int r = 0; r < NB; ++r) SX[r * LP + c] = Qc[base + (size_t)r * NB];
     }
     __syncwarp();
     if (on) {
@@ -465,7 +466,7 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_cgr_update(CgArgs a) {
         double2 acc = make_double2(0.0, 0.0);
 #pragma unroll
         for (int j = 0; j < NB; ++j) acc = cfma(SX[r * LP + j], u[j], acc);
-        a.Q[base + (size_t)r * NB] = acc;
+        Qc[base + (size_t)r * NB] = acc;
       }
     }
     __syncwarp();
@@ -608,7 +609,7 @@ __global__ void __launch_bounds__(32 * kEigWarps, 8) k_cgr_eig(CgArgs a, const d
       if (on) {
 #pragma unroll
         for (int r = 0; r < NB; ++r) {
-          q[r] = a.Q[base + (size_t)r * NB];
+          q[r] = q_cur(a)[base + (size_t)r * NB];
           SQ[r * LP + c] = q[r];
         }
       }

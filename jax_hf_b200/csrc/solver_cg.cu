@@ -37,7 +37,8 @@ int find_mu_internal(void* stream, int dtype, int method, int nk1, int nk2, int 
 
 struct CgScalars {
   int k, active, accepted, converged, k_base;
-  int first_ok;  // the first line-search trial was accepted: Q U(tau0) and eps are already in Vd / eps
+  int first_ok;  // the first line-search trial was accepted: Q U(tau0) and eps are already formed
+  int qsel;      // row path: the current Q is Vd (1) or the caller's Q buffer (0)
   double mu, E, E_prev, dE, grad_norm;
   double lam, pr_den, beta, tau0, tau_final, Omega0, E_fin;
 };
@@ -55,6 +56,13 @@ struct CgArgs {
 };
 
 __device__ __forceinline__ bool cg_active(const CgArgs& a) { return a.sc->active != 0; }
+// Row path (nb <= 8): Q alternates between the caller's buffer and Vd; the first
+// line-search trial writes Q U(tau0) into the other one and, when tau0 is
+// accepted, flips qsel instead of copying.  Finalize rotates it back into the
+// caller's buffer.
+__device__ __forceinline__ double2* q_cur(const CgArgs& a) { return a.sc->qsel ? a.Vd : a.Q; }
+__device__ __forceinline__ double2* q_alt(const CgArgs& a) { return a.sc->qsel ? a.Q : a.Vd; }
+__global__ void k_cg_qsel_reset(CgArgs a) { a.sc->qsel = 0; }
 
 }  // namespace hf
 
@@ -86,6 +94,7 @@ __global__ void k_cg_init(CgArgs a, const double2* __restrict__ P0, const double
     s->active = a.max_iter > 0 ? 1 : 0;
     s->accepted = 0;
     s->first_ok = 0;
+    s->qsel = 0;
     s->converged = 0;
     s->mu = 0.0;
     s->E = 0.0;
@@ -1107,7 +1116,9 @@ int CgSolver::launch_finalize() {
   if ((st = cg_density(r, s, 1))) return st;
   if ((st = cg_project(r, s))) return st;
   if ((st = cg_fock(r, s, false, nullptr))) return st;
-  if ((st = cg_eig(r, s, a.F, 1))) return st;
+  if ((st = cg_eig(r, s, a.F, 1))) return st;  // reads the current Q, writes the caller's buffer
+  k_cg_qsel_reset<<<1, 1, 0, s>>>(a);
+  HF_LAUNCH_CHECK("k_cg_qsel_reset");
   if ((st = cg_mu(r, s, cf->mu_maxiter, nullptr))) return st;
   if ((st = cg_density(r, s, 1))) return st;
   if ((st = cg_project(r, s))) return st;
