@@ -184,18 +184,37 @@ struct LineShape {
 // Per-thread twiddle rows of a line shape: the step-1 twiddles W_N^{n2 k1} of
 // part t (n2 = t + TPL i) at twf[t TS + i N1 + k1], and the inverse-step
 // twiddles W_N^{k1 m2} (k1 = t + TPL j) at twi[t TS + j N2 + m2].  Each table
-// holds TPL * TS entries; values are those of exp(-2 pi i e / N) from sincospi.
-template <class S, typename T>
-__device__ __forceinline__ void build_line_twiddles(cpx_t<T>* twf, cpx_t<T>* twi) {
-  for (int q = threadIdx.x; q < S::TPL * S::E; q += blockDim.x) {
+// holds TPL * TS entries; values are exp(-2 pi i e / N) from the compile-time
+// series (ct_cos2pi), so a pass copies its rows from a constant table in global
+// memory instead of evaluating 2 N FP64 sines in its prologue.
+template <class S>
+struct LineTwTable {
+  double v[2][S::TPL * S::E][2];  // [forward / inverse step][t E + r][re, im]
+};
+template <class S>
+constexpr LineTwTable<S> make_line_twiddles() {
+  LineTwTable<S> T{};
+  for (int q = 0; q < S::TPL * S::E; ++q) {
     const int t = q / S::E, r = q - t * S::E;
     const int ef = ((t + S::TPL * (r / S::N1)) * (r % S::N1)) % S::N;
     const int ei = ((t + S::TPL * (r / S::N2)) * (r % S::N2)) % S::N;
-    double sn, cs;
-    sincospi(-2.0 * (double)ef / (double)S::N, &sn, &cs);
-    twf[t * S::TS + r] = mk<cpx_t<T>>(cs, sn);
-    sincospi(-2.0 * (double)ei / (double)S::N, &sn, &cs);
-    twi[t * S::TS + r] = mk<cpx_t<T>>(cs, sn);
+    T.v[0][q][0] = ct_cos2pi(ef, S::N, false);
+    T.v[0][q][1] = -ct_cos2pi(ef, S::N, true);
+    T.v[1][q][0] = ct_cos2pi(ei, S::N, false);
+    T.v[1][q][1] = -ct_cos2pi(ei, S::N, true);
+  }
+  return T;
+}
+template <class S>
+__device__ constexpr LineTwTable<S> kLineTwiddles = make_line_twiddles<S>();
+
+template <class S, typename T>
+__device__ __forceinline__ void build_line_twiddles(cpx_t<T>* twf, cpx_t<T>* twi) {
+  const LineTwTable<S>& tab = kLineTwiddles<S>;
+  for (int q = threadIdx.x; q < S::TPL * S::E; q += blockDim.x) {
+    const int t = q / S::E, r = q - t * S::E;
+    twf[t * S::TS + r] = mk<cpx_t<T>>(tab.v[0][q][0], tab.v[0][q][1]);
+    twi[t * S::TS + r] = mk<cpx_t<T>>(tab.v[1][q][0], tab.v[1][q][1]);
   }
 }
 

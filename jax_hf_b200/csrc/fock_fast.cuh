@@ -20,6 +20,8 @@
 
 #include <cooperative_groups.h>
 
+#include <type_traits>
+
 #include "fft_reg.cuh"
 #include "fock_params.cuh"
 
@@ -187,7 +189,8 @@ __device__ __forceinline__ void stage_col(const FockParams& p, cpx_t<FT>* stage,
   cp_async_commit();
 }
 
-template <typename ST, typename FT, class S>
+// VREAL: the shifted V-hat is real (HF_FOCK_VR_REAL), one ST per entry.
+template <typename ST, typename FT, class S, bool VREAL>
 __global__ void __launch_bounds__(16 * S::TPL, 2) k_fast_col(const __grid_constant__ FockParams p) {
   pdl_launch_dependents();
   using SC = cpx_t<ST>;
@@ -201,7 +204,6 @@ __global__ void __launch_bounds__(16 * S::TPL, 2) k_fast_col(const __grid_consta
   const int nitems = p.ngroups * p.nk2;
   build_line_twiddles<S, FT>(twf, twi);
   const bool vr_scalar = (p.flags & HF_FOCK_VR_SCALAR) != 0;
-  const bool vr_real = (p.flags & HF_FOCK_VR_REAL) != 0;
   const size_t vstride = vr_scalar ? 1 : (size_t)p.nb2;
   const size_t rs = (size_t)p.nk2 * LS;
   int item = blockIdx.x;
@@ -213,21 +215,16 @@ __global__ void __launch_bounds__(16 * S::TPL, 2) k_fast_col(const __grid_consta
     const int g = item % p.ngroups, k2c = item / p.ngroups;
     const int c = s < LS ? p.chan[g * LS + s] : -1;
     const int vc = vr_scalar ? 0 : (c < 0 ? 0 : c);
-    // V-hat for the pattern-B frequencies of this thread, issued before the FFT
-    FT vr[S::E], vi[S::E];
+    // V-hat for the pattern-B frequencies of this thread, issued before the FFT and
+    // scaled only where it is used, so that the loads stay in flight across the transform
+    using VT = std::conditional_t<VREAL, ST, SC>;
+    VT vq[S::E];
 #pragma unroll
     for (int j = 0; j < S::E2; ++j)
 #pragma unroll
       for (int k2 = 0; k2 < S::N2; ++k2) {
         const size_t q = (size_t)S::idxB(t, j, k2) * p.nk2 + k2c;
-        if (vr_real) {
-          vr[j * S::N2 + k2] = (FT)((double)ld_stream(static_cast<const ST*>(p.VR) + q * vstride + vc) * p.scale);
-          vi[j * S::N2 + k2] = (FT)0;
-        } else {
-          const SC z = ld_stream(static_cast<const SC*>(p.VR) + q * vstride + vc);
-          vr[j * S::N2 + k2] = (FT)((double)z.x * p.scale);
-          vi[j * S::N2 + k2] = (FT)((double)z.y * p.scale);
-        }
+        vq[j * S::N2 + k2] = ld_stream(static_cast<const VT*>(p.VR) + q * vstride + vc);
       }
     cp_async_wait_all();
     FC x[S::E];
@@ -240,8 +237,14 @@ __global__ void __launch_bounds__(16 * S::TPL, 2) k_fast_col(const __grid_consta
     fwd_AB<S>(x, buf, twf + t * S::TS, t, s);
 #pragma unroll
     for (int e = 0; e < S::E; ++e) {
-      FC v = x[e];
-      x[e] = c < 0 ? mk<FC>(0.0, 0.0) : mk<FC>(v.x * vr[e] - v.y * vi[e], v.x * vi[e] + v.y * vr[e]);
+      const FC v = x[e];
+      if constexpr (VREAL) {
+        const FT w = (FT)((double)vq[e] * p.scale);
+        x[e] = c < 0 ? mk<FC>(0.0, 0.0) : mk<FC>(v.x * w, v.y * w);
+      } else {
+        const FT wr = (FT)((double)vq[e].x * p.scale), wi = (FT)((double)vq[e].y * p.scale);
+        x[e] = c < 0 ? mk<FC>(0.0, 0.0) : mk<FC>(v.x * wr - v.y * wi, v.x * wi + v.y * wr);
+      }
     }
     __syncthreads();  // buf is reused by the inverse transform
     inv_BA<S>(x, buf, twi + t * S::TS, t, s);
@@ -467,15 +470,21 @@ __global__ void __launch_bounds__(16 * S::TPL, 2) k_fast_row_inv_rows(const __gr
         if (c >= 0) st_stream(Sg + base + (size_t)(S::TPL * i + S::N2 * m1) * p.nb2, cadd(cvt<SC>(x[i * S::N1 + m1]), cab));
     cluster_wait();
 #pragma unroll
-    for (int i = 0; i < S::E1; ++i)
+    for (int i = 0; i < S::E1; ++i) {
+      // every partner load of the batch is issued before its F stores: a global store
+      // may alias the generic pbuf address, so interleaving them would serialise the
+      // distributed-shared-memory round trips
+      SC mo[S::N1];
+#pragma unroll
+      for (int m1 = 0; m1 < S::N1; ++m1) mo[m1] = pbuf[S::idxA(t, i, m1) * 16];
 #pragma unroll
       for (int m1 = 0; m1 < S::N1; ++m1) {
         const int e = i * S::N1 + m1;
-        const SC mo = pbuf[S::idxA(t, i, m1) * 16];
         if (c >= 0)
           st_stream(F + base + (size_t)(S::TPL * i + S::N2 * m1) * p.nb2,
-                    mk<SC>(0.5 * ((double)m[e].x + (double)mo.x) + hd, 0.5 * ((double)m[e].y - (double)mo.y)));
+                    mk<SC>(0.5 * ((double)m[e].x + (double)mo[m1].x) + hd, 0.5 * ((double)m[e].y - (double)mo[m1].y)));
       }
+    }
     cluster_arrive_relaxed();  // barrier B: this CTA's reads of the partners' buffers are done
     pending = true;
   }
@@ -525,9 +534,10 @@ int fast_fock(FockParams& p, cudaStream_t stream, bool* handled) {
   auto col = [&](auto shape) {
     using S = decltype(shape);
     constexpr size_t sm = fast_smem<S, FT>();
-    cudaFuncSetAttribute(k_fast_col<ST, FT, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    const int grid = persistent_grid(k_fast_col<ST, FT, S>, 16 * S::TPL, sm, p.ngroups * p.nk2);
-    const cudaError_t e = launch_pass(k_fast_col<ST, FT, S>, grid, 16 * S::TPL, sm, stream, p);
+    auto kern = (p.flags & HF_FOCK_VR_REAL) ? k_fast_col<ST, FT, S, true> : k_fast_col<ST, FT, S, false>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    const int grid = persistent_grid(kern, 16 * S::TPL, sm, p.ngroups * p.nk2);
+    const cudaError_t e = launch_pass(kern, grid, 16 * S::TPL, sm, stream, p);
     if (e != cudaSuccess) st = cuda_check(e, "k_fast_col");
   };
   auto inv = [&](auto shape) {
