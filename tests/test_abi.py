@@ -48,6 +48,19 @@ def test_reference_validation_errors_map_to_valueerror():
             _lib.HF_C128, _lib.FOCK_EXCHANGE | _lib.FOCK_PACKING, 4, 4, 2, C.byref(n)))
 
 
+def test_shape_limits_are_reported_on_the_host():
+    from jax_hf_b200 import _lib
+    n = C.c_size_t(0)
+    ex = _lib.FOCK_EXCHANGE
+    _lib.check(_lib.lib().hf_fock_workspace_size(_lib.HF_C128, ex, 3, 5, 32, C.byref(n)))
+    assert n.value > 0
+    with pytest.raises(_lib.HFError, match="nb > 32"):
+        _lib.check(_lib.lib().hf_fock_workspace_size(_lib.HF_C128, ex, 4, 4, 33, C.byref(n)))
+    for nk1, nk2, nb in ((0, 4, 2), (4, 0, 2), (4, 4, 0)):
+        with pytest.raises(ValueError, match="must be positive"):
+            _lib.check(_lib.lib().hf_fock_workspace_size(_lib.HF_C128, ex, nk1, nk2, nb, C.byref(n)))
+
+
 def test_status_strings():
     from jax_hf_b200 import _lib
     assert _lib.lib().hf_status_string(0) == b"ok"

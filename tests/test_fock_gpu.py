@@ -94,6 +94,12 @@ CASES = [
     (16, 9, 8, "layer", False, False),
     (96, 96, 4, "scalar", False, False),
     (13, 26, 3, "layer", True, False),
+    # band counts above the rows plan (tile slot groups / generic engine), up to the
+    # largest supported nb = 32
+    (10, 12, 9, "layer", True, False),
+    (12, 8, 12, "scalar", False, True),
+    (9, 6, 16, "layer", False, False),
+    (4, 6, 32, "layer", True, False),
 ]
 
 
