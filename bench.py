@@ -202,6 +202,34 @@ def run_ours(args, ws, rank, local):
         variants[name] = {"builds_per_s": round(1e6 / us, 1), "us_per_build": round(us, 2),
                           "achieved_gbs": round(nbytes / (us * 1e-6) / 1e9, 1)}
 
+    # a batch of independent densities through build_fock_batch: 12 distinct densities (k-shifted
+    # copies of the seeded density) and output sets cycled over the 64 builds of a step (1.4 GB,
+    # larger than L2; build i uses set i % 12 and stream i % streams, so a set is reused only 12
+    # builds later and on the same stream), h and V-hat shared by the batch as in a scan with one
+    # kernel; no flush.  The same batch on one stream isolates the gain
+    # of running builds on three streams.
+    bP = [torch.roll(P, shifts=(7 * r, 13 * r), dims=(0, 1)).contiguous() for r in range(12)]
+    bout = [(torch.empty_like(P), torch.empty_like(H), torch.empty_like(P)) for _ in range(12)]
+
+    def batch_rate(nstreams):
+        n = STEP_BUILDS
+        call = lambda: G.build_fock_batch([bP[i % 12] for i in range(n)], outs=[bout[i % 12] for i in range(n)],
+                                          streams=nstreams, **kw)
+        call()
+        torch.cuda.synchronize()
+        eb0, eb1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        eb0.record(stream)
+        call()
+        eb1.record(stream)
+        torch.cuda.synchronize()
+        us_b = 1e3 * eb0.elapsed_time(eb1) / n
+        return {"builds_per_s": round(1e6 / us_b, 1), "us_per_build": round(us_b, 2),
+                "achieved_gbs": round(alg_bytes(NK, NK, NB) / (us_b * 1e-6) / 1e9, 1)}
+
+    variants["c128_batch_1stream"] = batch_rate(1)
+    variants["c128_batch_3streams"] = batch_rate(3)
+    del bP, bout
+
     solves = run_solves(dev) if args.solves else None
     variants["solves"] = solves
 

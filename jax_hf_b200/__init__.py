@@ -7,13 +7,14 @@ call them, running hand-written CUDA kernels through the C ABI in
 """
 
 from .problem import HartreeFockKernel  # noqa: F401
-from .fock import build_fock, hf_energy, free_energy, occupation_entropy  # noqa: F401
+from .fock import build_fock, build_fock_batch, hf_energy, free_energy, occupation_entropy  # noqa: F401
 from .utils import find_chemical_potential, fermidirac, validate_electron_count, resample_kgrid  # noqa: F401
 from . import linalg  # noqa: F401
 
 __all__ = [
     "HartreeFockKernel",
     "build_fock",
+    "build_fock_batch",
     "hf_energy",
     "free_energy",
     "occupation_entropy",

@@ -161,8 +161,12 @@ _ws_cache: dict = {}
 
 
 def workspace(nbytes: int, device, tag: str = "ws") -> torch.Tensor:
-    """Caller-owned scratch from torch's caching allocator (256-byte aligned)."""
-    key = (tag, str(device))
+    """Caller-owned scratch from torch's caching allocator (256-byte aligned).
+
+    One buffer per (tag, device, current stream): calls on different streams may
+    run at the same time and never share scratch; calls on one stream are ordered.
+    """
+    key = (tag, str(device), torch.cuda.current_stream(device).cuda_stream)
     buf = _ws_cache.get(key)
     if buf is None or buf.numel() < nbytes:
         buf = torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=device)

@@ -381,3 +381,33 @@ def test_fock_hermitian_density_packing_192(cuda):
     assert rel(Sg, So) < TOL64
     assert rel(F, Fo) < TOL64
 
+
+
+@pytest.mark.parametrize("streams", [1, 2, 3])
+def test_build_fock_batch_matches_single_calls(cuda, streams):
+    """Independent builds spread over internal streams (each with its own scratch) give
+    exactly the single-call results; ``outs`` are filled in place."""
+    import jax_hf_b200 as G
+    prob, P, rng = _problem(48, 40, 8, "layer", 23)
+    HH = rng.normal(size=(8, 8))
+    ref = S.haar_density(48, 8, 5)[:48, :40] * 0.5
+    K, _ = _pair(prob, include_hartree=True, reference_density=np.ascontiguousarray(ref), hartree_matrix=HH + HH.T)
+    a = K.as_args()
+    kw = dict(h=a["h"], VR=a["VR"], refP=a["refP"], HH=a["HH"], w2d=K.w2d, include_exchange=True,
+              include_hartree=True, exchange_hermitian_channel_packing=a["exchange_hermitian_channel_packing"],
+              contact_g=a["contact_g"], contact_Oi=a["contact_Oi"], contact_Oj=a["contact_Oj"])
+    Ps = [torch.as_tensor(np.ascontiguousarray(S.haar_density(48, 8, 40 + i)[:48, :40]), device="cuda")
+          for i in range(5)]
+    single = [G.build_fock(Pi, **kw) for Pi in Ps]
+    outs = [tuple(torch.full_like(x, float("nan")) for x in r) for r in single]
+    got = G.build_fock_batch(Ps, outs=outs, streams=streams, **kw)
+    torch.cuda.synchronize()
+    for (s1, h1, f1), (s2, h2, f2), o in zip(single, got, outs):
+        assert torch.equal(s1, s2) and torch.equal(h1, h2) and torch.equal(f1, f2)
+        assert s2.data_ptr() == o[0].data_ptr() and f2.data_ptr() == o[2].data_ptr()
+    # without outs, and numpy inputs
+    got2 = G.build_fock_batch([Pi.cpu().numpy() for Pi in Ps], streams=streams, **kw)
+    for (s1, _, f1), (s2, _, f2) in zip(single, got2):
+        assert torch.equal(s1, s2) and torch.equal(f1, f2)
+    with pytest.raises(ValueError, match="outs has"):
+        G.build_fock_batch(Ps, outs=outs[:2], **kw)
