@@ -341,6 +341,31 @@ int hf_cg_solve(void* stream, const hf_cg_problem* problem, const hf_cg_config* 
                 void* Q, void* p, void* density, void* fock, double* hist_E, double* hist_grad,
                 double* scalars_out, void* workspace, size_t workspace_bytes);
 
+/* ---- SCF driver (complex128) ---------------------------------------------------
+ * Replaces jax_hf.reference_scf.solve_scf (reference_scf.py:124-365) for
+ * project_fn=None and the built-in Fock build: Roothaan iteration with linear
+ * mixing (acceleration 0), Pulay C-DIIS (1) or ODA (2), level shift and
+ * trust-radius clip; SCFConfig fields and defaults as reference_scf.py:31-63
+ * (diis_size <= 16).  The problem is described by an hf_cg_problem
+ * (sigma_buf / h_buf unused).  Inputs: P0 (nk1, nk2, nb, nb) complex128.
+ * Outputs: density and fock (device, as SCFResult.density_matrix /
+ * fock_matrix), the per-iteration histories hist_E, hist_D, hist_C (HOST
+ * float64, max_iter entries each, may be NULL) and scalars_out (HOST, 4
+ * float64): energy, chemical potential, iterations, converged.  Synchronises
+ * `stream` once per iteration (twice for ODA or a trust-radius clip). */
+typedef struct hf_scf_config {
+  int max_iter;
+  double density_tol, comm_tol, mixing, level_shift;
+  int acceleration; /* 0 linear, 1 diis, 2 oda */
+  int diis_size, diis_start;
+  double diis_damping, trust_radius;
+} hf_scf_config;
+
+int hf_scf_workspace_size(const hf_cg_problem* problem, const hf_scf_config* config, size_t* bytes);
+int hf_scf_solve(void* stream, const hf_cg_problem* problem, const hf_scf_config* config, const void* P0,
+                 void* density, void* fock, double* hist_E, double* hist_D, double* hist_C, double* scalars_out,
+                 void* workspace, size_t workspace_bytes);
+
 /* ---- Reverse mode (complex128) -------------------------------------------------
  * The reference differentiates build_fock / hf_energy / free_energy with
  * jax.grad (fock.py:18-129 under jax autodiff); these are the hand-written

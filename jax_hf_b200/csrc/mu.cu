@@ -34,7 +34,10 @@ struct MuArgs {
   const double* mu0;
   double* out;
   const int* active;  // optional device flag: return at once when *active == 0
+  int cache;          // n <= 4 x threads of the cluster: (eps, w) kept in shared memory
 };
+// (eps, w) entries of one thread in the shared-memory cache (layout [u][thread])
+constexpr int kMuCacheU = 4;
 
 template <typename RT>
 __device__ __forceinline__ double load_eps(const MuArgs& a, int e) {
@@ -72,11 +75,14 @@ __device__ __forceinline__ void cluster_sum2(cg::cluster_group& cl, double& x, d
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   if (lane == 0) { wsm[2 * wid] = x; wsm[2 * wid + 1] = y; }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    double sx = 0.0, sy = 0.0;
-    for (int i = 0; i < nw; ++i) { sx += wsm[2 * i]; sy += wsm[2 * i + 1]; }
-    slots[parity][0] = sx;
-    slots[parity][1] = sy;
+  if (wid == 0) {  // the warp partials, reduced by one warp
+    double sx = lane < nw ? wsm[2 * lane] : 0.0, sy = lane < nw ? wsm[2 * lane + 1] : 0.0;
+    sx = warp_sum(sx);
+    sy = warp_sum(sy);
+    if (lane == 0) {
+      slots[parity][0] = sx;
+      slots[parity][1] = sy;
+    }
   }
   cl.sync();
   double tx = 0.0, ty = 0.0;
@@ -124,8 +130,31 @@ __global__ void __launch_bounds__(kMuThreads) k_find_mu(const MuArgs a) {
   cg::cluster_group cl = cg::this_cluster();
   __shared__ double slots[3][2];
   __shared__ double wsm[64];
+  extern __shared__ double2 mu_cache[];  // a.cache: (eps, w) of this thread's elements, [u][thread]
   const int gt = cl.block_rank() * blockDim.x + threadIdx.x;
   const int gs = cl.num_blocks() * blockDim.x;
+  // every pass visits this thread's elements in the same order, from shared memory when
+  // they fit (each thread reads back only what it stored: no barrier), else from L2
+  if (a.cache) {
+#pragma unroll
+    for (int u = 0; u < kMuCacheU; ++u) {
+      const int e = gt + u * gs;
+      mu_cache[u * blockDim.x + threadIdx.x] =
+          e < a.n ? make_double2(load_eps<RT>(a, e), load_w<RT>(a, e)) : make_double2(0.0, 0.0);
+    }
+  }
+  auto visit = [&](auto&& f) {
+    if (a.cache) {
+#pragma unroll
+      for (int u = 0; u < kMuCacheU; ++u)
+        if (gt + u * gs < a.n) {
+          const double2 c = mu_cache[u * blockDim.x + threadIdx.x];
+          f(c.x, c.y);
+        }
+    } else {
+      for_each_eps<RT, kMuCacheU>(a, gt, gs, f);
+    }
+  };
 
   // Method 2 with a warm start: the min/max pass also forms N and Z at mu0, which
   // are the first Newton evaluation whenever mu0 lies inside the bracket.
@@ -134,7 +163,7 @@ __global__ void __launch_bounds__(kMuThreads) k_find_mu(const MuArgs a) {
   const double Tf = fmax(a.T, 1e-12);
   double mn = INFINITY, mx = -INFINITY, N0 = 0.0, Z0 = 0.0;
   if (fuse_first) {
-    for_each_eps<RT, 4>(a, gt, gs, [&](double v, double w) {
+    visit([&](double v, double w) {
       mn = fmin(mn, v);
       mx = fmax(mx, v);
       const double p = expit((mu0v - v) / Tf);
@@ -142,7 +171,7 @@ __global__ void __launch_bounds__(kMuThreads) k_find_mu(const MuArgs a) {
       Z0 += w * (p * (1.0 - p)) / Tf;
     });
   } else {
-    for_each_eps<RT, 4>(a, gt, gs, [&](double v, double) {
+    visit([&](double v, double) {
       mn = fmin(mn, v);
       mx = fmax(mx, v);
     });
@@ -163,7 +192,7 @@ __global__ void __launch_bounds__(kMuThreads) k_find_mu(const MuArgs a) {
     for (int it = 0; it < a.maxiter; ++it) {
       const double mid = 0.5 * (lo + hi);
       double cnt = 0.0, dummy = 0.0;
-      for_each_eps<RT, 4>(a, gt, gs, [&](double ev, double w) { cnt += w * expit(-(ev - mid) / Td); });
+      visit([&](double ev, double w) { cnt += w * expit(-(ev - mid) / Td); });
       cluster_sum2(cl, cnt, dummy, slots, wsm, parity);
       parity ^= 1;
       const double nlo = (cnt > a.target) ? lo : mid;
@@ -194,7 +223,7 @@ __global__ void __launch_bounds__(kMuThreads) k_find_mu(const MuArgs a) {
         N = N0;
         Z = Z0;
       } else {
-        for_each_eps<RT, 4>(a, gt, gs, [&](double ev, double w) {
+        visit([&](double ev, double w) {
           const double p = expit((mu - ev) / Tj);
           N += w * p;
           Z += w * (p * (1.0 - p)) / Tj;
@@ -217,7 +246,7 @@ __global__ void __launch_bounds__(kMuThreads) k_find_mu(const MuArgs a) {
     }
     if (a.method == 1) {
       double N = 0.0, dummy = 0.0;
-      for_each_eps<RT, 4>(a, gt, gs, [&](double ev, double w) { N += w * expit((mu - ev) / Tj); });
+      visit([&](double ev, double w) { N += w * expit((mu - ev) / Tj); });
       cluster_sum2(cl, N, dummy, slots, wsm, parity);
       parity ^= 1;
       if (fabs(N - a.target) > 1e-12) mu = 0.5 * (lo + hi);
@@ -291,10 +320,23 @@ int hf::find_mu_internal(void* stream, int dtype, int method, int nk1, int nk2, 
     }
     if (csize > mc) csize = mc;
   }
+  a.cache = a.n <= kMuCacheU * csize * kMuThreads ? 1 : 0;
+  const size_t cache_bytes = (size_t)kMuCacheU * kMuThreads * sizeof(double2);
+  if (a.cache) {
+    static bool smem_set[2][64] = {};  // per (precision, device)
+    int dev = 0;
+    HF_CUDA(cudaGetDevice(&dev));
+    bool& done = smem_set[single ? 1 : 0][dev & 63];
+    if (!done) {
+      const void* fn = single ? (const void*)k_find_mu<float> : (const void*)k_find_mu<double>;
+      HF_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cache_bytes));
+      done = true;
+    }
+  }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(csize, 1, 1);
   cfg.blockDim = dim3(kMuThreads, 1, 1);
-  cfg.dynamicSmemBytes = 0;
+  cfg.dynamicSmemBytes = a.cache ? cache_bytes : 0;
   cfg.stream = static_cast<cudaStream_t>(stream);
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;

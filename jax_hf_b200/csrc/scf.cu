@@ -1,0 +1,342 @@
+// Native SCF driver (reference_scf.py:124-365, solve_scf with project_fn=None
+// and the built-in Fock build): Roothaan iteration with linear mixing, Pulay
+// C-DIIS or ODA, level shift and trust-radius clip, complex128.
+//
+// Every array step is one of the library's device operations (Fock build,
+// energy, Jacobi eigh, bisection mu, occupations, density, residuals, DIIS
+// Gram matrix, extrapolation).  The host keeps the loop's scalar decisions, as
+// the reference does in its traced loop, and reads them in one small
+// device->host copy per iteration (residual sums, energy, Gram matrix; plus
+// the second energy of an ODA step and the step norm of a trust-radius clip).
+// The bordered (n+1)^2 DIIS system is solved on the host by LU with partial
+// pivoting (the algorithm of LAPACK gesv behind numpy.linalg.solve).
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+
+namespace hf {
+namespace {
+
+struct ScfLayout {
+  size_t off[24];
+  size_t total;
+};
+
+enum {
+  kDH, kSG, kH, kF, kPN, kDELTA, kUPD, kFX, kFD, kFH, kPD, kSTEP, kV, kEV, kSH, kOCC, kRH, kFHIST, kSCAL,
+  kFOCKWS, kREDWS, kOPSWS, kNBUF
+};
+
+// device scalar block (float64): mu_raw, mu, E, E_new, sums[3], red[1], gram[21], coeff[n]
+constexpr int kSMuRaw = 0, kSMu = 1, kSE = 2, kSEnew = 3, kSSums = 4, kSRed = 7, kSGram = 8, kSCoeff = 29;
+
+size_t scf_layout(const hf_cg_problem& pb, const hf_scf_config& cf, size_t fock_ws, size_t red_ws, size_t ops_ws,
+                  ScfLayout& L) {
+  const size_t nk = (size_t)pb.nk1 * pb.nk2, nb = pb.nb, nq = nk * nb * nb, nv = nk * nb;
+  const size_t nh = cf.acceleration == 1 ? (size_t)cf.diis_size : 1;
+  size_t sizes[kNBUF] = {};
+  sizes[kDH] = sizes[kSG] = sizes[kF] = sizes[kPN] = sizes[kDELTA] = sizes[kUPD] = nq * 16;
+  sizes[kFX] = sizes[kFD] = sizes[kFH] = sizes[kPD] = sizes[kSTEP] = sizes[kV] = nq * 16;
+  sizes[kH] = nb * nb * 16;
+  sizes[kEV] = sizes[kSH] = sizes[kOCC] = nv * 8;
+  sizes[kRH] = nh * nq * 16;
+  sizes[kFHIST] = cf.acceleration == 1 ? nh * nq * 16 : 256;
+  sizes[kSCAL] = (kSCoeff + nh + 8) * 8;
+  sizes[kFOCKWS] = fock_ws;
+  sizes[kREDWS] = red_ws;
+  sizes[kOPSWS] = ops_ws;
+  size_t o = 0;
+  for (int i = 0; i < kNBUF; ++i) {
+    L.off[i] = o;
+    o += align_up(sizes[i] > 0 ? sizes[i] : 256, 256);
+  }
+  L.total = o;
+  return o;
+}
+
+// Solves A x = b (n <= 16) by LU with partial pivoting (first maximum |a| as the
+// pivot row, as idamax); returns false on an exactly singular pivot.
+bool lu_solve(std::vector<double> A, std::vector<double> b, int n, std::vector<double>& x) {
+  for (int j = 0; j < n; ++j) {
+    int p = j;
+    double best = std::fabs(A[j * n + j]);
+    for (int i = j + 1; i < n; ++i)
+      if (std::fabs(A[i * n + j]) > best) { best = std::fabs(A[i * n + j]); p = i; }
+    if (A[p * n + j] == 0.0) return false;
+    if (p != j) {
+      for (int c = 0; c < n; ++c) std::swap(A[j * n + c], A[p * n + c]);
+      std::swap(b[j], b[p]);
+    }
+    const double inv = 1.0 / A[j * n + j];
+    for (int i = j + 1; i < n; ++i) {
+      const double l = A[i * n + j] * inv;
+      A[i * n + j] = l;
+      for (int c = j + 1; c < n; ++c) A[i * n + c] -= l * A[j * n + c];
+    }
+  }
+  for (int i = 0; i < n; ++i)  // L y = P b (unit diagonal)
+    for (int c = 0; c < i; ++c) b[i] -= A[i * n + c] * b[c];
+  x.assign(n, 0.0);
+  for (int i = n - 1; i >= 0; --i) {
+    double s = b[i];
+    for (int c = i + 1; c < n; ++c) s -= A[i * n + c] * x[c];
+    x[i] = s / A[i * n + i];
+  }
+  return true;
+}
+
+struct Scf {
+  cudaStream_t s;
+  const hf_cg_problem* pb;
+  const hf_scf_config* cf;
+  unsigned char* base;
+  ScfLayout L;
+  size_t fock_ws, red_ws;
+  int nk, nb;
+  size_t nq;
+
+  template <typename T>
+  T* at(int i) const { return reinterpret_cast<T*>(base + L.off[i]); }
+  double* scal() const { return at<double>(kSCAL); }
+
+  int herm_axpby(double a, const void* x, double b, const void* y, void* out) {
+    return hf_axpby(s, (size_t)nk, nb, a, x, b, y, 1, out);
+  }
+  int fock(const void* P, void* Sg, void* H, void* F) {
+    return hf_fock_build(s, HF_C128, pb->fock_flags, pb->nk1, pb->nk2, nb, P, pb->h, pb->VR, pb->refP, pb->HH,
+                         pb->w2d, pb->n_contact, pb->contact_g, pb->contact_Oi, pb->contact_Oj, Sg, H, F,
+                         at<void>(kFOCKWS), fock_ws);
+  }
+  int energy(const void* P, const void* Sg, const void* H, double* E) {
+    // H from hf_fock_build is one nb x nb matrix for all k (H_mode 1); zero without Hartree
+    return hf_energy(s, HF_C128, pb->nk1, pb->nk2, nb, P, pb->h, Sg, H, 1, pb->w2d, E, at<void>(kREDWS), red_ws);
+  }
+  // reference_scf.py:87-96: eigh, bisection mu, level shift, occupations, density
+  int density_from_fock(const void* F, void* P_out) {
+    int st;
+    double* sc = scal();
+    if ((st = hf_eigh(s, HF_C128, nk, nb, F, at<double>(kEV), at<void>(kV)))) return st;
+    if ((st = hf_find_mu(s, HF_C128, 0, nk, 1, nb, at<double>(kEV), pb->w2d, pb->n_electrons, pb->T, 0, nullptr,
+                         sc + kSMuRaw)))
+      return st;
+    const double* shifted = at<double>(kEV);
+    const double* mu = sc + kSMuRaw;
+    if (cf->level_shift != 0.0) {
+      if ((st = hf_fermi(s, (size_t)nk * nb, at<double>(kEV), sc + kSMuRaw, pb->T, 2, cf->level_shift,
+                         at<double>(kSH))))
+        return st;
+      if ((st = hf_find_mu(s, HF_C128, 0, nk, 1, nb, at<double>(kSH), pb->w2d, pb->n_electrons, pb->T, 0,
+                           nullptr, sc + kSMu)))
+        return st;
+      shifted = at<double>(kSH);
+      mu = sc + kSMu;
+    } else {
+      HF_CUDA(cudaMemcpyAsync(sc + kSMu, sc + kSMuRaw, sizeof(double), cudaMemcpyDeviceToDevice, s));
+    }
+    if ((st = hf_fermi(s, (size_t)nk * nb, shifted, mu, pb->T, 0, 0.0, at<double>(kOCC)))) return st;
+    return hf_density_from_Qp(s, HF_C128, nk, nb, at<void>(kV), at<double>(kOCC), P_out);
+  }
+  // reference_scf.py:78-84: herm(density) -> build -> energy -> next density
+  int build_and_occupy(const void* dens, void* F, void* Pn) {
+    int st;
+    if ((st = herm_axpby(1.0, dens, 0.0, nullptr, at<void>(kDH)))) return st;
+    if ((st = fock(at<void>(kDH), at<void>(kSG), at<void>(kH), F))) return st;
+    if ((st = energy(at<void>(kDH), at<void>(kSG), at<void>(kH), scal() + kSE))) return st;
+    return density_from_fock(F, Pn);
+  }
+  int read(double* host, const double* dev, int n) {
+    HF_CUDA(cudaMemcpyAsync(host, dev, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    HF_CUDA(cudaStreamSynchronize(s));
+    return HF_OK;
+  }
+};
+
+}  // namespace
+}  // namespace hf
+
+using namespace hf;
+
+static int scf_check(const hf_cg_problem* pb, const hf_scf_config* cf) {
+  if (!pb || !cf) return fail(HF_ERR_INVALID, "hf_scf: null problem or config");
+  if (pb->nk1 < 1 || pb->nk2 < 1 || pb->nb < 1 || pb->nb > 32)
+    return fail(HF_ERR_INVALID, "hf_scf: bad mesh or band count");
+  if (cf->max_iter <= 0) return fail(HF_ERR_INVALID, "max_iter must be positive");
+  if (cf->acceleration < 0 || cf->acceleration > 2)
+    return fail(HF_ERR_INVALID, "SCFConfig.acceleration must be 'linear', 'diis', or 'oda'");
+  if (cf->diis_size <= 0) return fail(HF_ERR_INVALID, "diis_size must be positive");
+  if (cf->acceleration == 1 && cf->diis_size > 16) return fail(HF_ERR_UNSUPPORTED, "hf_scf: diis_size > 16");
+  return HF_OK;
+}
+
+static int scf_sizes(const hf_cg_problem* pb, const hf_scf_config* cf, size_t* fock_ws, size_t* red_ws,
+                     size_t* ops_ws) {
+  int st;
+  if ((st = hf_fock_workspace_size(HF_C128, pb->fock_flags, pb->nk1, pb->nk2, pb->nb, fock_ws))) return st;
+  if ((st = hf_reduce_workspace_size(pb->nk1, pb->nk2, pb->nb, red_ws))) return st;
+  return hf_ops_workspace_size(ops_ws);
+}
+
+extern "C" int hf_scf_workspace_size(const hf_cg_problem* pb, const hf_scf_config* cf, size_t* bytes) {
+  int st;
+  if ((st = scf_check(pb, cf))) return st;
+  if (!bytes) return fail(HF_ERR_INVALID, "hf_scf_workspace_size: null output");
+  size_t f = 0, r = 0, o = 0;
+  if ((st = scf_sizes(pb, cf, &f, &r, &o))) return st;
+  ScfLayout L;
+  *bytes = scf_layout(*pb, *cf, f, r, o, L);
+  return HF_OK;
+}
+
+extern "C" int hf_scf_solve(void* stream, const hf_cg_problem* pb, const hf_scf_config* cf, const void* P0,
+                            void* density, void* fock, double* hist_E, double* hist_D, double* hist_C,
+                            double* scalars_out, void* workspace, size_t workspace_bytes) {
+  int st;
+  if ((st = scf_check(pb, cf))) return st;
+  if (!P0 || !density || !fock || !scalars_out || !workspace)
+    return fail(HF_ERR_INVALID, "hf_scf_solve: null buffer");
+  Scf S;
+  S.s = static_cast<cudaStream_t>(stream);
+  S.pb = pb;
+  S.cf = cf;
+  S.base = static_cast<unsigned char*>(workspace);
+  S.nk = pb->nk1 * pb->nk2;
+  S.nb = pb->nb;
+  S.nq = (size_t)S.nk * pb->nb * pb->nb;
+  size_t ops_ws = 0;
+  if ((st = scf_sizes(pb, cf, &S.fock_ws, &S.red_ws, &ops_ws))) return st;
+  if (scf_layout(*pb, *cf, S.fock_ws, S.red_ws, ops_ws, S.L) > workspace_bytes)
+    return fail(HF_ERR_INVALID, "hf_scf_solve: workspace too small");
+  const cudaStream_t s = S.s;
+  const int nk = S.nk, nb = S.nb;
+  const size_t nq = S.nq, qbytes = nq * 16;
+  const bool diis = cf->acceleration == 1, oda = cf->acceleration == 2;
+  const int nh = diis ? cf->diis_size : 1;
+  const double wsum = std::fmax(pb->weight_sum, 1e-30);
+  double* sc = S.scal();
+  void* ops = S.at<void>(kOPSWS);
+  const double* w2d = static_cast<const double*>(pb->w2d);
+
+  HF_CUDA(cudaMemcpyAsync(density, P0, qbytes, cudaMemcpyDeviceToDevice, s));
+  if (diis) {
+    HF_CUDA(cudaMemsetAsync(S.at<void>(kRH), 0, (size_t)nh * qbytes, s));
+    HF_CUDA(cudaMemsetAsync(S.at<void>(kFHIST), 0, (size_t)nh * qbytes, s));
+  }
+  std::vector<double> hv(kSCoeff + 8, 0.0);
+  int k = 0;
+  bool converged = false;
+  while (k < cf->max_iter && !converged) {
+    void* F = S.at<void>(kF);
+    void* Pn = S.at<void>(kPN);
+    if ((st = S.build_and_occupy(density, F, Pn))) return st;
+    void* R_out = diis ? (void*)(S.at<unsigned char>(kRH) + (size_t)(k % nh) * qbytes) : (void*)S.at<void>(kRH);
+    if ((st = hf_scf_residuals(s, nk, nb, F, density, Pn, w2d, R_out, S.at<void>(kDELTA), sc + kSSums, ops)))
+      return st;
+    if (diis) {
+      HF_CUDA(cudaMemcpyAsync(S.at<unsigned char>(kFHIST) + (size_t)(k % nh) * qbytes, F, qbytes,
+                              cudaMemcpyDeviceToDevice, s));
+      if (nh <= 6) {
+        if ((st = hf_gram(s, nh, nq, nk, nb, S.at<void>(kRH), w2d, sc + kSGram, ops))) return st;
+      }
+    }
+    if ((st = S.read(hv.data(), sc, kSCoeff))) return st;
+    const double E_host = hv[kSE];
+    const double d_res = std::sqrt(hv[kSSums] / wsum), c_res = std::sqrt(hv[kSSums + 1] / wsum);
+    converged = d_res <= cf->density_tol && c_res <= cf->comm_tol;
+    void* updated = S.at<void>(kUPD);
+    if (diis) {
+      // B_ij = sum_k w Re tr(R_i^H R_j) over every history slot (zeros where unused)
+      std::vector<double> B((size_t)nh * nh, 0.0);
+      if (nh <= 6) {
+        int q = 0;
+        for (int i = 0; i < nh; ++i)
+          for (int j = i; j < nh; ++j, ++q) B[i * nh + j] = B[j * nh + i] = hv[kSGram + q];
+      } else {
+        for (int i = 0; i < nh; ++i)
+          for (int j = i; j < nh; ++j) {
+            if ((st = hf_jdot(s, (size_t)nk, nb, S.at<unsigned char>(kRH) + (size_t)i * qbytes,
+                              S.at<unsigned char>(kRH) + (size_t)j * qbytes, w2d, nullptr, nullptr, nullptr,
+                              sc + kSRed, ops)))
+              return st;
+            double v = 0.0;
+            if ((st = S.read(&v, sc + kSRed, 1))) return st;
+            B[i * nh + j] = B[j * nh + i] = v;
+          }
+      }
+      double bmax = 0.0;
+      for (double v : B) bmax = std::fmax(bmax, std::fabs(v));
+      bmax = std::fmax(bmax, 1e-30);
+      const int count = k + 1 < nh ? k + 1 : nh;
+      const int m = nh + 1;
+      std::vector<double> A((size_t)m * m, 0.0), rhs(m, 0.0), sol;
+      for (int i = 0; i < nh; ++i) {
+        const double act = i < count ? 1.0 : 0.0;
+        for (int j = 0; j < nh; ++j) A[i * m + j] = B[i * nh + j] / bmax;
+        A[i * m + i] += 1.0 - act;
+        A[i * m + nh] = -act;
+        A[nh * m + i] = -act;
+      }
+      rhs[nh] = -1.0;
+      bool ok = lu_solve(A, rhs, m, sol);
+      if (ok)
+        for (double v : sol) ok = ok && std::isfinite(v);
+      const int start = cf->diis_start > 2 ? cf->diis_start : 2;
+      if (count >= start && ok) {
+        // from pageable memory: the values are staged before the call returns
+        HF_CUDA(cudaMemcpyAsync(sc + kSCoeff, sol.data(), nh * sizeof(double), cudaMemcpyHostToDevice, s));
+        if ((st = hf_lincomb(s, nh, nq, nq, S.at<void>(kFHIST), sc + kSCoeff, S.at<void>(kFX)))) return st;
+        const void* Fx = S.at<void>(kFX);
+        const double damp = std::fmin(std::fmax(cf->diis_damping, 0.0), 1.0);
+        if (damp != 1.0) {
+          if ((st = hf_axpby(s, (size_t)nk, nb, damp, Fx, 1.0 - damp, F, 0, S.at<void>(kFD)))) return st;
+          Fx = S.at<void>(kFD);
+        }
+        if ((st = S.herm_axpby(1.0, Fx, 0.0, nullptr, S.at<void>(kFH)))) return st;
+        if ((st = S.density_from_fock(S.at<void>(kFH), updated))) return st;
+      } else {
+        if ((st = S.herm_axpby(1.0, density, cf->mixing, S.at<void>(kDELTA), updated))) return st;
+      }
+    } else if (oda) {
+      if ((st = S.fock(Pn, S.at<void>(kSG), S.at<void>(kH), S.at<void>(kFX)))) return st;
+      if ((st = S.energy(Pn, S.at<void>(kSG), S.at<void>(kH), sc + kSEnew))) return st;
+      double E_new = 0.0;
+      if ((st = S.read(&E_new, sc + kSEnew, 1))) return st;
+      const double c1 = hv[kSSums + 2];
+      const double c2 = (E_new - E_host) - c1;
+      double lam;
+      if (c2 > 1e-12) lam = std::fmin(std::fmax(-c1 / (2.0 * c2), 0.0), 1.0);
+      else lam = c1 < 0.0 ? 1.0 : 0.0;
+      if ((st = S.herm_axpby(1.0, density, lam, S.at<void>(kDELTA), updated))) return st;
+    } else {
+      if ((st = S.herm_axpby(1.0, density, cf->mixing, S.at<void>(kDELTA), updated))) return st;
+    }
+    if (cf->trust_radius > 0.0) {  // reference_scf.py:333-339
+      if ((st = hf_axpby(s, (size_t)nk, nb, 1.0, updated, -1.0, density, 0, S.at<void>(kSTEP)))) return st;
+      if ((st = hf_jdot(s, (size_t)nk, nb, S.at<void>(kSTEP), S.at<void>(kSTEP), w2d, nullptr, nullptr,
+                        nullptr, sc + kSRed, ops)))
+        return st;
+      double red = 0.0;
+      if ((st = S.read(&red, sc + kSRed, 1))) return st;
+      const double sn = std::sqrt(red / wsum);
+      if (sn > cf->trust_radius) {
+        const double scale = cf->trust_radius / std::fmax(sn, 1e-30);
+        if ((st = S.herm_axpby(1.0, density, scale, S.at<void>(kSTEP), updated))) return st;
+      }
+    }
+    HF_CUDA(cudaMemcpyAsync(density, converged ? Pn : updated, qbytes, cudaMemcpyDeviceToDevice, s));
+    if (hist_E) hist_E[k] = E_host;
+    if (hist_D) hist_D[k] = d_res;
+    if (hist_C) hist_C[k] = c_res;
+    ++k;
+  }
+  // final build at the returned density (reference_scf.py:345-347)
+  if ((st = S.build_and_occupy(density, fock, S.at<void>(kPN)))) return st;
+  double fin[3] = {0.0, 0.0, 0.0};
+  if ((st = S.read(fin, sc, 3))) return st;
+  scalars_out[0] = fin[kSE];
+  scalars_out[1] = fin[kSMu];
+  scalars_out[2] = (double)k;
+  scalars_out[3] = converged ? 1.0 : 0.0;
+  return HF_OK;
+}

@@ -24,6 +24,11 @@ from .linalg import eigh, density_from_Qp
 from .utils import validate_electron_count
 
 
+# solve_scf runs the library's SCF driver (hf_scf_solve) when no project_fn or custom
+# fock_build_fn is given; False keeps every call on the Python loop below.
+USE_NATIVE = True
+
+
 @dataclass(frozen=True)
 class SCFConfig:
     """reference_scf.py:31-63 (same fields, defaults and validation)."""
@@ -110,6 +115,8 @@ def solve_scf(kernel, P0, n_electrons: float, *, config: SCFConfig | None = None
     ops = _Ops(dev, nk1, nk2, nb)
     project = cfg.project_fn
     validate_electron_count(w2d, nb, n_electrons, context="n_electrons")
+    if USE_NATIVE and fock_build_fn is None and project is None and (cfg.acceleration != "diis" or cfg.diis_size <= 16):
+        return _solve_scf_native(kernel, P0, n_electrons, cfg)
     a = kernel.as_args()
     VR = a["VR"] if kernel.dtype == cd else (a["VR"].to(cd) if a["VR"].is_complex() else a["VR"].to(torch.float64))
     fock_kw = dict(h=h, VR=VR, refP=kernel.refP if kernel.dtype == cd else kernel.refP.to(cd), HH=kernel.HH.double(),
@@ -254,6 +261,65 @@ def solve_scf(kernel, P0, n_electrons: float, *, config: SCFConfig | None = None
                      chemical_potential=mu_fin, iterations=n_iter, converged=bool(converged), message=message,
                      history={"E": np.asarray(hE), "density_residual": np.asarray(hD),
                               "commutator_residual": np.asarray(hC)})
+
+
+class _ScfConfig(C.Structure):
+    _fields_ = [("max_iter", C.c_int), ("density_tol", C.c_double), ("comm_tol", C.c_double),
+                ("mixing", C.c_double), ("level_shift", C.c_double), ("acceleration", C.c_int),
+                ("diis_size", C.c_int), ("diis_start", C.c_int), ("diis_damping", C.c_double),
+                ("trust_radius", C.c_double)]
+
+
+def _solve_scf_native(kernel, P0, n_electrons, cfg):
+    """solve_scf through the library's SCF driver (hf_scf_solve): the same steps as the
+    loop above, sequenced in C++ with one small device->host read per iteration."""
+    from .solver import KernelC128, _CgProblem
+
+    L = _lib.lib()
+    if not getattr(L, "_scf_bound", False):
+        L.hf_scf_workspace_size.argtypes = [C.POINTER(_CgProblem), C.POINTER(_ScfConfig), C.POINTER(C.c_size_t)]
+        L.hf_scf_workspace_size.restype = C.c_int
+        L.hf_scf_solve.argtypes = [C.c_void_p, C.POINTER(_CgProblem), C.POINTER(_ScfConfig), C.c_void_p,
+                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.c_size_t]
+        L.hf_scf_solve.restype = C.c_int
+        L._scf_bound = True
+    dev = kernel.device
+    cd = torch.complex128
+    kc = KernelC128(kernel)
+    pb = kc.problem(n_electrons)
+    acc = {"linear": 0, "diis": 1, "oda": 2}[cfg.acceleration]
+    sc = _ScfConfig(int(cfg.max_iter), float(cfg.density_tol), float(cfg.comm_tol), float(cfg.mixing),
+                    float(cfg.level_shift), acc, int(cfg.diis_size), int(cfg.diis_start), float(cfg.diis_damping),
+                    float(cfg.trust_radius))
+    need = C.c_size_t(0)
+    _lib.check(L.hf_scf_workspace_size(C.byref(pb), C.byref(sc), C.byref(need)))
+    ws = _lib.workspace(need.value, dev, "scf")
+    P0d = torch.as_tensor(P0).to(dev, cd).contiguous()
+    density = torch.empty_like(P0d)
+    fock = torch.empty_like(P0d)
+    m = int(cfg.max_iter)
+    hist = np.zeros((3, m))
+    out = np.zeros(4)
+    dp = lambda a: a.ctypes.data_as(C.c_void_p)
+    _lib.check(L.hf_scf_solve(_lib.stream_ptr(dev), C.byref(pb), C.byref(sc), P0d.data_ptr(), density.data_ptr(),
+                              fock.data_ptr(), dp(hist[0]), dp(hist[1]), dp(hist[2]), dp(out), ws.data_ptr(),
+                              ws.numel()))
+    n_iter = int(out[2])
+    converged = bool(out[3] != 0.0)
+    hE, hD, hC = hist[0, :n_iter].copy(), hist[1, :n_iter].copy(), hist[2, :n_iter].copy()
+    if converged:
+        message = f"converged in {n_iter} iterations"
+    else:
+        dr = hD[-1] if n_iter > 0 else float("nan")
+        cr = hC[-1] if n_iter > 0 else float("nan")
+        message = f"stopped after {n_iter} iterations (density_res={dr:.3e}, comm_res={cr:.3e})"
+    out_c = kernel.dtype
+    return SCFResult(density_matrix=density.to(out_c), fock_matrix=fock.to(out_c),
+                     energy=torch.tensor(float(out[0]), dtype=torch.float64, device=dev),
+                     chemical_potential=torch.tensor(float(out[1]), dtype=torch.float64, device=dev),
+                     iterations=n_iter, converged=converged, message=message,
+                     history={"E": hE, "density_residual": hD, "commutator_residual": hC})
 
 
 def _linear(ops, density, delta, mixing, project, proj_herm):

@@ -72,9 +72,14 @@ SCF_CASES = [
 ]
 
 
+@pytest.mark.parametrize("engine", ["native", "python"])
 @pytest.mark.parametrize("name,model,ne,cfg", SCF_CASES, ids=[c[0] for c in SCF_CASES])
-def test_scf_matches_oracle(cuda, name, model, ne, cfg):
+def test_scf_matches_oracle(cuda, monkeypatch, name, model, ne, cfg, engine):
+    """Both drivers: the library's hf_scf_solve (default) and the Python loop over the
+    same device operations (what solve_scf runs with a project_fn or fock_build_fn)."""
+    from jax_hf_b200 import reference_scf
     from jax_hf_b200.reference_scf import SCFConfig, solve_scf
+    monkeypatch.setattr(reference_scf, "USE_NATIVE", engine == "native")
     if model == "scf24":
         p = S.scf_diis_24()
         kw = p.kernel_kwargs()
@@ -100,6 +105,31 @@ def test_scf_matches_oracle(cuda, name, model, ne, cfg):
     # history slot holds an exactly zero commutator (P0 = 0), so only the first steps are compared
     n = min(len(r.history["E"]), len(ro["history"]["E"]), 3 if cfg.get("acceleration") == "diis" else 6)
     np.testing.assert_allclose(r.history["E"][:n], ro["history"]["E"][:n], rtol=1e-9, atol=1e-9)
+
+
+@pytest.mark.parametrize("name,model,ne,cfg", SCF_CASES, ids=[c[0] for c in SCF_CASES])
+def test_native_scf_driver_matches_python_loop(cuda, monkeypatch, name, model, ne, cfg):
+    """hf_scf_solve sequences the same device operations as the Python loop: identical
+    iteration counts and histories up to the round-off of the host DIIS solve."""
+    from jax_hf_b200 import reference_scf
+    from jax_hf_b200.reference_scf import SCFConfig, solve_scf
+    kw = S.scf_diis_24().kernel_kwargs() if model == "scf24" else _dirac()
+    K, _ = _kernels(kw)
+    P0 = torch.zeros(np.asarray(kw["hamiltonian"]).shape, dtype=torch.complex128, device="cuda")
+    res = {}
+    for native in (True, False):
+        monkeypatch.setattr(reference_scf, "USE_NATIVE", native)
+        res[native] = solve_scf(K, P0, ne, config=SCFConfig(**cfg))
+    a, b = res[True], res[False]
+    assert a.converged == b.converged
+    assert abs(a.iterations - b.iterations) <= (3 if cfg.get("acceleration") == "diis" else 0)
+    n = min(a.iterations, b.iterations, 3 if cfg.get("acceleration") == "diis" else 10 ** 6)
+    np.testing.assert_allclose(a.history["E"][:n], b.history["E"][:n], rtol=1e-12, atol=1e-13)
+    np.testing.assert_allclose(a.history["density_residual"][:n], b.history["density_residual"][:n],
+                               rtol=1e-9, atol=1e-14)
+    assert abs(float(a.energy) - float(b.energy)) <= 1e-10 * max(1.0, abs(float(b.energy)))
+    assert (a.density_matrix - b.density_matrix).abs().max().item() < 1e-6
+    assert a.message.split()[0] == b.message.split()[0]
 
 
 def test_scf_config_validation():
