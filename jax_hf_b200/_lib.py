@@ -85,6 +85,8 @@ _SIGS = {
     "hf_cg_workspace_size": ([vp, vp, psz], i32),
     "hf_cg_solve": ([vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, sz], i32),
     "hf_cg_batch_workspace_size": ([vp, i32, vp, psz], i32),
+    "hf_scf_workspace_size": ([vp, vp, psz], i32),
+    "hf_scf_solve": ([vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, sz], i32),
     "hf_fock_vjp_workspace_size": ([i32, u32, i32, i32, i32, psz], i32),
     "hf_fock_build_vjp": ([vp, i32, u32, i32, i32, i32, vp, vp, vp, vp, vp, vp, sz], i32),
     "hf_energy_vjp": ([vp, i32, i32, i32, vp, vp, vp, vp, i32, vp, f64, vp, vp, vp], i32),
