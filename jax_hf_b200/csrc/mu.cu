@@ -291,7 +291,11 @@ int hf::find_mu_internal(void* stream, int dtype, int method, int nk1, int nk2, 
   a.eps = eps; a.w = weights;
   a.n = nk1 * nk2 * nb; a.nb = nb; a.method = method; a.maxiter = maxiter;
   a.target = n_electrons; a.T = T; a.mu0 = mu0; a.out = mu_out; a.active = active;
-  int csize = (a.n + 4 * kMuThreads - 1) / (4 * kMuThreads);
+  // bisection (54 FP64-bound passes of an exp and a division per element): about one
+  // element per thread, so small meshes spread over several SMs; the Newton variants
+  // (3-25 passes, bound by the cluster barrier of each pass): up to four per thread
+  const int per_thread = method == 0 ? 1 : kMuCacheU;
+  int csize = (a.n + per_thread * kMuThreads - 1) / (per_thread * kMuThreads);
   if (csize < 1) csize = 1;
   if (csize > kMuMaxCluster) csize = kMuMaxCluster;
   if (csize > 8) {  // beyond the portable 8: only as large as the device can co-schedule

@@ -31,9 +31,22 @@ __global__ void k_sum_partials(const double* __restrict__ part, int nblk, int ns
   const int q = threadIdx.x;
   if (q >= ns) return;
   KSum t;
-  for (int b = 0; b < nblk; ++b) {
-    t.add(part[((size_t)b * ns + q) * 2]);
-    t.add(part[((size_t)b * ns + q) * 2 + 1]);
+  // block order as before; the loads of a batch are issued before its compensated adds
+  constexpr int U = 8;
+  for (int b0 = 0; b0 < nblk; b0 += U) {
+    double v[2 * U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const bool in = b0 + u < nblk;
+      v[2 * u] = in ? part[((size_t)(b0 + u) * ns + q) * 2] : 0.0;
+      v[2 * u + 1] = in ? part[((size_t)(b0 + u) * ns + q) * 2 + 1] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (b0 + u < nblk) {
+        t.add(v[2 * u]);
+        t.add(v[2 * u + 1]);
+      }
   }
   out[q] = t.value();
 }
