@@ -7,6 +7,11 @@ occupations, residuals/commutators, DIIS Gram matrix, extrapolation); the
 loop's scalar decisions are taken on the host from a few float64 reductions per
 iteration, as the reference does in its traced loop.  The (N+1)^2 bordered DIIS
 system is solved on the host with LAPACK (numpy), like jnp.linalg.solve on CPU.
+
+Without a project_fn or a custom fock_build_fn, solve_scf runs the same loop in
+the library's C++ driver (hf_scf_solve), which issues the same device operations
+and reads the loop's scalars once per iteration; the Python loop below serves the
+hooks (and USE_NATIVE = False).
 """
 
 from __future__ import annotations
