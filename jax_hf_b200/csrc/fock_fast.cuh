@@ -189,9 +189,10 @@ __device__ __forceinline__ void stage_col(const FockParams& p, cpx_t<FT>* stage,
   cp_async_commit();
 }
 
-// VREAL: the shifted V-hat is real (HF_FOCK_VR_REAL), one ST per entry.
+// VREAL: the shifted V-hat is real (HF_FOCK_VR_REAL), one ST per entry.  With an FP32
+// transform the shared memory of a CTA is half as large, so three CTAs share an SM.
 template <typename ST, typename FT, class S, bool VREAL>
-__global__ void __launch_bounds__(16 * S::TPL, 2) k_fast_col(const __grid_constant__ FockParams p) {
+__global__ void __launch_bounds__(16 * S::TPL, sizeof(FT) == 4 ? 3 : 2) k_fast_col(const __grid_constant__ FockParams p) {
   pdl_launch_dependents();
   using SC = cpx_t<ST>;
   using FC = cpx_t<FT>;
