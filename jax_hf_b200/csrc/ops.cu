@@ -117,19 +117,26 @@ __global__ void k_scf_residuals(int nk, int nb, const double2* __restrict__ F, c
 
 // ------------------------------------------------------- DIIS Gram matrix --
 // B[i][j] = sum_k w_k Re tr(R_i^H R_j) for i, j < n (R_i at R + i*stride)
-__global__ void k_gram(int n, size_t stride, size_t len, int nb2, const double2* __restrict__ R,
+// N (history slots) is a template parameter so that every loop has a compile-time
+// trip count and the N (N + 1) / 2 accumulators stay in registers.
+template <int N>
+__global__ void k_gram(size_t stride, size_t len, int nb2, const double2* __restrict__ R,
                        const double* __restrict__ w, double* part) {
   __shared__ double red[64];
-  KSum acc[kOpsMaxSums];
-  const int np = n * (n + 1) / 2;
+  constexpr int np = N * (N + 1) / 2;
+  KSum acc[np];
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < len; e += (size_t)gridDim.x * blockDim.x) {
     const double wk = w[e / nb2];
-    double2 r[6];
-    for (int i = 0; i < n; ++i) r[i] = R[i * stride + e];
+    double2 r[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) r[i] = R[i * stride + e];
     int q = 0;
-    for (int i = 0; i < n; ++i)
-      for (int j = i; j < n; ++j, ++q) acc[q].add(wk * (r[i].x * r[j].x + r[i].y * r[j].y));
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+      for (int j = i; j < N; ++j, ++q) acc[q].add(wk * (r[i].x * r[j].x + r[i].y * r[j].y));
   }
+#pragma unroll
   for (int q = 0; q < np; ++q) {
     KSum rr = block_reduce(acc[q], red);
     if (threadIdx.x == 0) {
@@ -434,7 +441,12 @@ extern "C" int hf_gram(void* stream, int n, size_t stride, int nk, int nb, const
   if (n < 1 || n > 6 || !R || !w || !B_out || !ws) return fail(HF_ERR_INVALID, "hf_gram: 1 <= n <= 6");
   const size_t len = (size_t)nk * nb * nb;
   const int g = nblocks(len);
-  k_gram<<<g, kOpsThreads, 0, HF_S>>>(n, stride, len, nb * nb, (const double2*)R, w, (double*)ws);
+  switch (n) {
+#define HF_GRAM(N) \
+  case N: k_gram<N><<<g, kOpsThreads, 0, HF_S>>>(stride, len, nb * nb, (const double2*)R, w, (double*)ws); break;
+    HF_GRAM(1) HF_GRAM(2) HF_GRAM(3) HF_GRAM(4) HF_GRAM(5) HF_GRAM(6)
+#undef HF_GRAM
+  }
   return finish(HF_S, (double*)ws, g, n * (n + 1) / 2, B_out);
 }
 
