@@ -57,6 +57,12 @@ extern "C" {
  * the rows plan would apply (nb <= 8 without packing); a schedule choice, the
  * result is the same to rounding. */
 #define HF_FOCK_TILE_PLAN (1u << 9)
+/* Run the rows plan (nb in {4, 8}, register mesh lengths, 16-byte aligned
+ * operands) on the bulk-copy pipeline: one persistent CTA per SM, a ring of
+ * shared-memory stages filled by tensor / bulk copies, Sigma and the
+ * hermitised F in separate passes.  A schedule choice (the result is the same
+ * to rounding); the autotuner times it as a candidate. */
+#define HF_FOCK_PIPE (1u << 10)
 const char* hf_last_error(void);
 const char* hf_status_string(int status);
 int hf_version(void);
@@ -105,9 +111,9 @@ int hf_fock_build_static_scratch(void* stream, int dtype, unsigned flags, int nk
  * no counterpart in the reference, whose FFTs are XLA's).  Same arguments as
  * hf_fock_build, plus reps (timed builds
  * per candidate, >= 1), chosen (out: the engine flags picked) and us (out,
- * may be NULL: mean microseconds per build of each candidate, in the order
- * default schedule / HF_FOCK_TILE_PLAN / HF_FOCK_GENERIC_FFT, -1 for a
- * candidate that does not apply).  Every candidate runs on the caller's
+ * may be NULL, 4 entries: mean microseconds per build of each candidate, in
+ * the order default schedule / HF_FOCK_TILE_PLAN / HF_FOCK_GENERIC_FFT /
+ * HF_FOCK_PIPE, -1 for a candidate that does not apply).  Every candidate runs on the caller's
  * buffers (one untimed build, then reps timed with CUDA events on `stream`),
  * the fastest is stored in a process-wide table keyed by (device, dtype,
  * flags, nk1, nk2, nb), and the outputs hold the winner's result on return.
@@ -123,6 +129,14 @@ int hf_fock_autotune(void* stream, int dtype, unsigned flags, int nk1, int nk2, 
                      unsigned* chosen, float* us);
 /* Forgets every stored autotuner choice. */
 int hf_fock_autotune_reset(void);
+
+/* Device fault word of the pipelined Fock passes on the current device (no
+ * counterpart in the reference).  Every wait of those kernels on an mbarrier
+ * is bounded (2 s); one that runs out records a nonzero code (2: a consumer
+ * group waiting for a stage's copy, 3: waiting for the copy to be issued) and
+ * the kernel returns without finishing the build.  Synchronises the device, copies
+ * the word to *code and, when clear != 0, resets it to zero. */
+int hf_fock_fault_status(int* code, int clear);
 
 /* Periodic linear resampling of the two leading axes of an (n1, n2, ...)
  * array on a centered k-grid (k = 0 at index n / 2) to (m1, m2, ...):

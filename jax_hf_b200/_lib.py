@@ -31,6 +31,7 @@ FOCK_HAS_REFP = 1 << 6
 FOCK_GENERIC_FFT = 1 << 7
 FOCK_SYM_V = 1 << 8
 FOCK_TILE_PLAN = 1 << 9
+FOCK_PIPE = 1 << 10
 
 vp, i32, u32, f64, sz = C.c_void_p, C.c_int, C.c_uint, C.c_double, C.c_size_t
 pf64 = C.POINTER(C.c_double)
@@ -46,6 +47,7 @@ _SIGS = {
     "hf_fock_autotune": ([vp, i32, u32, i32, i32, i32, vp, vp, vp, vp, vp, vp, i32, vp, vp, vp,
                           vp, vp, vp, vp, sz, i32, C.POINTER(C.c_uint), C.POINTER(C.c_float)], i32),
     "hf_fock_autotune_reset": ([], i32),
+    "hf_fock_fault_status": ([C.POINTER(C.c_int), i32], i32),
     "hf_resample_kgrid": ([vp, i32, i32, i32, i32, i32, C.c_longlong, vp, vp], i32),
     "hf_resample_density": ([vp, i32, i32, i32, i32, i32, i32, vp, vp], i32),
     "hf_sym_group_average": ([vp, i32, i32, i32, i32, vp, vp, i32, vp, i32, vp, i32, i32, vp, vp, vp], i32),

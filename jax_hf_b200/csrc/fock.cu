@@ -471,7 +471,9 @@ static int launch_fock(FockParams& p, cudaStream_t stream, bool need_consts) {
   }
   if (!(p.flags & HF_FOCK_GENERIC_FFT)) {
     bool handled = false;
-    const int st = fast_fock<ST, FT>(p, stream, &handled);
+    int st = pipe_fock<ST, FT>(p, stream, &handled);
+    if (st != HF_OK || handled) return st;
+    st = fast_fock<ST, FT>(p, stream, &handled);
     if (st != HF_OK || handled) return st;
   }
   if (exch) {
@@ -485,9 +487,34 @@ static int launch_fock(FockParams& p, cudaStream_t stream, bool need_consts) {
   return HF_OK;
 }
 
+// ------------------------------------------------------------ fault word -----
+// Written by the bounded waits of the pipelined passes (fock_pipe.cuh).  Its
+// address is looked up once per device; the lookup does not survive a reset of
+// the device's primary context (cudaDeviceReset) within the process.
+__device__ int g_fock_fault;
+static std::mutex g_fault_mu;
+static std::map<int, int*> g_fault_ptr;
+
+static int fault_word(int** out) {
+  int dev = 0;
+  HF_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_fault_mu);
+  auto it = g_fault_ptr.find(dev);
+  if (it == g_fault_ptr.end()) {
+    void* ptr = nullptr;
+    HF_CUDA(cudaGetSymbolAddress(&ptr, g_fock_fault));
+    it = g_fault_ptr.emplace(dev, static_cast<int*>(ptr)).first;
+  }
+  *out = it->second;
+  return HF_OK;
+}
+
 // ------------------------------------------------------------ autotuner -----
 // Engine flags chosen by hf_fock_autotune per (device, dtype, flags, nk1, nk2, nb).
-constexpr unsigned kEngineFlags = HF_FOCK_TILE_PLAN | HF_FOCK_GENERIC_FFT;
+constexpr unsigned kEngineFlags = HF_FOCK_TILE_PLAN | HF_FOCK_GENERIC_FFT | HF_FOCK_PIPE;
+constexpr int kTuneCands = 4;
+// default schedule, 2x2-tile slot plan, generic engine, bulk-copy pipeline
+constexpr unsigned kTuneCand[kTuneCands] = {0u, HF_FOCK_TILE_PLAN, HF_FOCK_GENERIC_FFT, HF_FOCK_PIPE};
 using TuneKey = std::tuple<int, int, unsigned, int, int, int>;
 static std::mutex g_tune_mu;
 static std::map<TuneKey, unsigned> g_tune;
@@ -517,8 +544,7 @@ extern "C" int hf_fock_workspace_size(int dtype, unsigned flags, int nk1, int nk
   if (st) return st;
   // every schedule the autotuner may pick (they differ only in the slot plan)
   size_t most = 0;
-  const unsigned cands[3] = {0u, HF_FOCK_TILE_PLAN, HF_FOCK_GENERIC_FFT};
-  for (unsigned e : cands) {
+  for (unsigned e : kTuneCand) {
     if ((flags & kEngineFlags) && e != 0) continue;
     SlotPlan sp;
     if ((st = get_plan(dtype, flags | e, nk1, nk2, nb, sp))) return st;
@@ -582,6 +608,7 @@ static int fock_build_exact(void* stream, int dtype, unsigned flags, int nk1, in
   p.cg = contact_g; p.cOi = contact_Oi; p.cOj = contact_Oj;
   p.Sigma = Sigma; p.F = F; p.Hout = H;
   p.active = active;
+  if ((st = fault_word(&p.fault))) return st;
   char* ws = static_cast<char*>(workspace);
   p.scratch = ws + wl.scratch;
   const bool need_consts = (flags & HF_FOCK_HARTREE) || n_contact > 0;
@@ -625,11 +652,11 @@ extern "C" int hf_fock_autotune(void* stream, int dtype, unsigned flags, int nk1
   if (reps < 1) return fail(HF_ERR_INVALID, "reps must be >= 1");
   if (flags & kEngineFlags) return fail(HF_ERR_INVALID, "hf_fock_autotune chooses the engine flags itself");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const unsigned cands[3] = {0u, HF_FOCK_TILE_PLAN, HF_FOCK_GENERIC_FFT};
-  // the tile candidate only differs from the default where the rows plan applies
+  const unsigned* cands = kTuneCand;
+  // the tile and pipeline candidates only differ from the default where the rows plan applies
   SlotPlan sp0;
   if ((st = get_plan(dtype, flags, nk1, nk2, nb, sp0))) return st;
-  float times[3] = {-1.f, -1.f, -1.f};
+  float times[kTuneCands] = {-1.f, -1.f, -1.f, -1.f};
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   HF_CUDA(cudaEventCreate(&e0));
   if (cudaEventCreate(&e1) != cudaSuccess) {
@@ -637,8 +664,8 @@ extern "C" int hf_fock_autotune(void* stream, int dtype, unsigned flags, int nk1
     return fail(HF_ERR_CUDA, "cudaEventCreate failed");
   }
   int best = -1;
-  for (int c = 0; c < 3 && st == HF_OK; ++c) {
-    if (c == 1 && !sp0.rows) continue;
+  for (int c = 0; c < kTuneCands && st == HF_OK; ++c) {
+    if ((c == 1 || c == 3) && !sp0.rows) continue;
     const unsigned f = flags | cands[c];
     auto run = [&] {
       return fock_build_exact(stream, dtype, f, nk1, nk2, nb, P, h, VR, refP, HH, w2d, n_contact, contact_g,
@@ -670,7 +697,18 @@ extern "C" int hf_fock_autotune(void* stream, int dtype, unsigned flags, int nk1
   if (st != HF_OK) return st;
   if (chosen) *chosen = cands[best];
   if (us)
-    for (int c = 0; c < 3; ++c) us[c] = times[c];
+    for (int c = 0; c < kTuneCands; ++c) us[c] = times[c];
+  return HF_OK;
+}
+
+extern "C" int hf_fock_fault_status(int* code, int clear) {
+  if (!code) return hf::fail(HF_ERR_INVALID, "code is NULL");
+  int* w = nullptr;
+  int st = hf::fault_word(&w);
+  if (st) return st;
+  HF_CUDA(cudaDeviceSynchronize());
+  HF_CUDA(cudaMemcpy(code, w, sizeof(int), cudaMemcpyDeviceToHost));
+  if (clear) HF_CUDA(cudaMemset(w, 0, sizeof(int)));
   return HF_OK;
 }
 

@@ -1,6 +1,8 @@
 // Parameters of the Fock-build kernels (shared by the generic and fast paths).
 #pragma once
 
+#include <cuda.h>
+
 #include "fft_engine.cuh"
 
 namespace hf {
@@ -33,6 +35,10 @@ struct FockParams {
   double* hdiag;      // [nb] Hartree diagonal
   const int* active;  // optional device flag: kernels return at once when *active == 0
   int rows_plan;      // slot groups are whole matrix rows; partner = (group << 8) | slot
+  int pipe_ns;        // stages of the pipelined passes (set per launch)
+  int* fault;         // device word: a bounded wait of a pipelined pass that ran out records a code here
+  CUtensorMap tmap_row;  // pipelined row pass: P as [nk1 nk2][nb^2] 4-byte words, box = SL channels x nk2 k-points
+  CUtensorMap tmap_col;  // pipelined column pass: scratch as [group nk1][nk2][SL], box = one column
   int16_t chan[kMaxSlotTable];
   int16_t partner[kMaxSlotTable];
 };
@@ -66,5 +72,8 @@ inline bool fast_length(int n) {
 // Launches the fast passes when both mesh lengths have a fast shape.
 template <typename ST, typename FT>
 int fast_fock(FockParams& p, cudaStream_t stream, bool* handled);
+// Launches the bulk-copy pipelined passes (fock_pipe.cuh) where they apply.
+template <typename ST, typename FT>
+int pipe_fock(FockParams& p, cudaStream_t stream, bool* handled);
 
 }  // namespace hf

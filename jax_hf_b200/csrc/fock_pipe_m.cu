@@ -1,0 +1,7 @@
+// Pipelined Fock passes, storage double / FFT float (instantiation unit).
+#include "fock_fast.cuh"
+#include "fock_pipe.cuh"
+
+namespace hf {
+template int pipe_fock<double, float>(FockParams&, cudaStream_t, bool*);
+}  // namespace hf

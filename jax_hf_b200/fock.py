@@ -14,7 +14,9 @@ Differences in form, not in value:
   inputs in FP32; everything else stays FP64.
 * ``engine="generic"`` (extension, for testing) forces the shared-memory
   Stockham engine instead of the register FFT of the specialised mesh lengths;
-  ``engine="tile"`` forces the 2x2-tile slot groups in the register engine.
+  ``engine="tile"`` forces the 2x2-tile slot groups in the register engine;
+  ``engine="pipe"`` runs the bulk-copy pipelined passes (nb in {4, 8} on
+  register lengths; the default schedule elsewhere).
 * ``autotune=True`` (extension) times the schedules that apply to this shape
   (``hf_fock_autotune``), keeps the fastest for every later build of the same
   shape and flags (solver drivers included) and records the timings in
@@ -126,6 +128,8 @@ def build_fock(P, *, h, VR, refP, HH, w2d, include_exchange: bool, include_hartr
         flags |= _lib.FOCK_GENERIC_FFT
     elif engine is not None and str(engine).lower() == "tile":
         flags |= _lib.FOCK_TILE_PLAN
+    elif engine is not None and str(engine).lower() == "pipe":
+        flags |= _lib.FOCK_PIPE
     if fft_precision is not None and str(fft_precision).lower() in ("fp32", "float32", "single"):
         if cdt == torch.complex128:
             flags |= _lib.FOCK_FFT_FP32
@@ -154,10 +158,11 @@ def build_fock(P, *, h, VR, refP, HH, w2d, include_exchange: bool, include_hartr
             _lib.ptr(cOj), Sigma.data_ptr(), H.data_ptr(), F.data_ptr(), ws.data_ptr(), ws.numel())
     if autotune:
         chosen = _lib.C.c_uint(0)
-        us = (_lib.C.c_float * 3)()
+        us = (_lib.C.c_float * 4)()
         _lib.check(_lib.lib().hf_fock_autotune(*args, int(autotune_reps), _lib.C.byref(chosen), us))
-        names = ("default", "tile", "generic")
-        pick = {0: "default", _lib.FOCK_TILE_PLAN: "tile", _lib.FOCK_GENERIC_FFT: "generic"}[chosen.value]
+        names = ("default", "tile", "generic", "pipe")
+        pick = {0: "default", _lib.FOCK_TILE_PLAN: "tile", _lib.FOCK_GENERIC_FFT: "generic",
+                _lib.FOCK_PIPE: "pipe"}[chosen.value]
         last_autotune.clear()
         last_autotune.update(shape=(nk1, nk2, nb), flags=flags, chosen=pick,
                              us={n: float(v) for n, v in zip(names, us) if v >= 0})
