@@ -67,7 +67,12 @@ __device__ __forceinline__ void for_each_eps(const MuArgs& a, int gt, int gs, F&
   }
 }
 
-// cluster-wide sum of (x, y); every thread of every CTA receives the total.
+// Cluster-wide sum of (x, y); every thread of every CTA receives the total.
+// Each CTA publishes its block sum in its `slots`; after the cluster barrier,
+// lane r of warp 0 reads CTA r's slot (one distributed-shared-memory read per
+// lane, all in flight together) and warp 0 reduces them with a fixed shuffle
+// tree, so every CTA obtains bit-identical totals.  slots is double-buffered by
+// `parity`: a CTA may publish the next pass while a slower one still reads this.
 __device__ __forceinline__ void cluster_sum2(cg::cluster_group& cl, double& x, double& y,
                                              double (*slots)[2], double* wsm, int parity) {
   x = warp_sum(x);
@@ -85,15 +90,20 @@ __device__ __forceinline__ void cluster_sum2(cg::cluster_group& cl, double& x, d
     }
   }
   cl.sync();
-  double tx = 0.0, ty = 0.0;
-  const unsigned nbk = cl.num_blocks();
-  for (unsigned r = 0; r < nbk; ++r) {
-    double(*rs)[2] = cl.map_shared_rank(slots, r);
-    tx += rs[parity][0];
-    ty += rs[parity][1];
+  if (wid == 0) {
+    double tx = 0.0, ty = 0.0;
+    if (lane < (int)cl.num_blocks()) {
+      double(*rs)[2] = cl.map_shared_rank(slots, lane);
+      tx = rs[parity][0];
+      ty = rs[parity][1];
+    }
+    tx = warp_sum(tx);
+    ty = warp_sum(ty);
+    if (lane == 0) { wsm[64] = tx; wsm[65] = ty; }
   }
-  x = tx;
-  y = ty;
+  __syncthreads();
+  x = wsm[64];
+  y = wsm[65];
 }
 
 __device__ __forceinline__ void cluster_minmax(cg::cluster_group& cl, double& mn, double& mx,
@@ -105,21 +115,34 @@ __device__ __forceinline__ void cluster_minmax(cg::cluster_group& cl, double& mn
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   if (lane == 0) { wsm[2 * wid] = mn; wsm[2 * wid + 1] = mx; }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    double a = wsm[0], b = wsm[1];
-    for (int i = 1; i < nw; ++i) { a = fmin(a, wsm[2 * i]); b = fmax(b, wsm[2 * i + 1]); }
-    slots[2][0] = a;
-    slots[2][1] = b;
+  if (wid == 0) {
+    double a = lane < nw ? wsm[2 * lane] : INFINITY, b = lane < nw ? wsm[2 * lane + 1] : -INFINITY;
+    for (int off = 16; off > 0; off >>= 1) {
+      a = fmin(a, __shfl_xor_sync(0xffffffffu, a, off));
+      b = fmax(b, __shfl_xor_sync(0xffffffffu, b, off));
+    }
+    if (lane == 0) {
+      slots[2][0] = a;
+      slots[2][1] = b;
+    }
   }
   cl.sync();
-  double a = INFINITY, b = -INFINITY;
-  for (unsigned r = 0; r < cl.num_blocks(); ++r) {
-    double(*rs)[2] = cl.map_shared_rank(slots, r);
-    a = fmin(a, rs[2][0]);
-    b = fmax(b, rs[2][1]);
+  if (wid == 0) {
+    double a = INFINITY, b = -INFINITY;
+    if (lane < (int)cl.num_blocks()) {
+      double(*rs)[2] = cl.map_shared_rank(slots, lane);
+      a = rs[2][0];
+      b = rs[2][1];
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+      a = fmin(a, __shfl_xor_sync(0xffffffffu, a, off));
+      b = fmax(b, __shfl_xor_sync(0xffffffffu, b, off));
+    }
+    if (lane == 0) { wsm[64] = a; wsm[65] = b; }
   }
-  mn = a;
-  mx = b;
+  __syncthreads();
+  mn = wsm[64];
+  mx = wsm[65];
 }
 
 __device__ __forceinline__ double expit(double x) { return 1.0 / (1.0 + exp(-x)); }
@@ -129,7 +152,7 @@ __global__ void __launch_bounds__(kMuThreads) k_find_mu(const MuArgs a) {
   if (a.active && !*a.active) return;  // uniform across the cluster: no barrier is skipped by a subset
   cg::cluster_group cl = cg::this_cluster();
   __shared__ double slots[3][2];
-  __shared__ double wsm[64];
+  __shared__ double wsm[66];
   extern __shared__ double2 mu_cache[];  // a.cache: (eps, w) of this thread's elements, [u][thread]
   const int gt = cl.block_rank() * blockDim.x + threadIdx.x;
   const int gs = cl.num_blocks() * blockDim.x;
