@@ -3,10 +3,11 @@
 Reads ``tests/data/meshgrid_regression_case_v1.npz`` of the reference (jax_hf)
 and keeps the fields that pin ``build_fock`` + ``hf_energy`` (12x12 mesh, 4
 bands, complex64, exchange + Hartree + reference density).  Run from the repo
-root:  ``python tests/golden/make_golden.py /root/reference``.
+root with the reference checkout's root directory as the one required argument:
+``python tests/golden/make_golden.py <reference-root>``.
 """
 
-import sys
+import argparse
 from pathlib import Path
 
 import numpy as np
@@ -26,4 +27,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("reference_root", help="root directory of the jax_hf checkout (holds tests/data/)")
+    main(ap.parse_args().reference_root)
