@@ -1,11 +1,13 @@
 // Chemical potential: mu such that sum_k w_k sum_j f(eps_kj - mu) = N.
 //
-// One thread-block cluster (up to 8 CTAs x 1024 threads) runs the whole root
-// find: every iteration each CTA reduces its slice, publishes the partial in
-// its shared memory, one cluster barrier, and every CTA then sums all partials
-// through distributed shared memory in rank order.  All CTAs therefore hold
-// bit-identical (mu, lo, hi) and take identical branches; no global-memory
-// round trip and no second launch per iteration.
+// One thread-block cluster (up to 16 CTAs) runs the whole root find: every
+// iteration each CTA reduces its slice, publishes the partial in its shared
+// memory, one cluster barrier, and warp 0 of every CTA then reads all partials
+// through distributed shared memory and reduces them with a fixed shuffle tree.
+// All CTAs therefore hold bit-identical (mu, lo, hi) and take identical
+// branches; no global-memory round trip and no second launch per iteration.
+// The bisection evaluates four levels per pass (the 15 midpoints of the next
+// four levels in one reduction, then the four decisions in order).
 //
 // Methods (reference):
 //   0  _find_mu_bisection  utils.py:353-382 (maxiter 54 f64 / 30 f32)
@@ -17,6 +19,11 @@
 // there, moving mu by at most a few ulp).
 #include <cooperative_groups.h>
 
+#include <climits>
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "common.cuh"
 
 namespace cg = cooperative_groups;
@@ -25,6 +32,7 @@ namespace hf {
 
 constexpr int kMuThreads = 1024;
 constexpr int kMuMaxCluster = 16;  // non-portable size, used when the device schedules it
+constexpr int kBisLevels = 4;  // bisection levels per pass of the 256-thread variant
 
 struct MuArgs {
   const void* eps;
@@ -106,6 +114,43 @@ __device__ __forceinline__ void cluster_sum2(cg::cluster_group& cl, double& x, d
   y = wsm[65];
 }
 
+// Cluster-wide sums of K values (as cluster_sum2); v[] holds this thread's terms
+// on entry and the totals on return.  bsm: 32 * K + K doubles, slots: [2][K].
+template <int K>
+__device__ __forceinline__ void cluster_sum_n(cg::cluster_group& cl, double (&v)[K], double (*slots)[K], double* bsm,
+                                              int parity) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    v[j] = warp_sum(v[j]);
+    if (lane == 0) bsm[wid * K + j] = v[j];
+  }
+  __syncthreads();
+  if (wid == 0) {
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      double t = lane < nw ? bsm[lane * K + j] : 0.0;
+      t = warp_sum(t);
+      if (lane == 0) slots[parity][j] = t;
+    }
+  }
+  cl.sync();
+  if (wid == 0) {
+    double(*rs)[K] = lane < (int)cl.num_blocks() ? cl.map_shared_rank(slots, lane) : nullptr;
+    double t[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) t[j] = rs ? rs[parity][j] : 0.0;
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      t[j] = warp_sum(t[j]);
+      if (lane == 0) bsm[32 * K + j] = t[j];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < K; ++j) v[j] = bsm[32 * K + j];
+}
+
 __device__ __forceinline__ void cluster_minmax(cg::cluster_group& cl, double& mn, double& mx,
                                                double (*slots)[2], double* wsm) {
   for (int off = 16; off > 0; off >>= 1) {
@@ -147,12 +192,17 @@ __device__ __forceinline__ void cluster_minmax(cg::cluster_group& cl, double& mn
 
 __device__ __forceinline__ double expit(double x) { return 1.0 / (1.0 + exp(-x)); }
 
-template <typename RT>
-__global__ void __launch_bounds__(kMuThreads) k_find_mu(const MuArgs a) {
+// BT threads per CTA; the bisection evaluates L levels per pass (L = 4 for the
+// 256-thread variant, 1 for the 1024-thread variant, whose register budget is 64).
+template <typename RT, int BT>
+__global__ void __launch_bounds__(BT) k_find_mu(const MuArgs a) {
+  constexpr int L = BT <= 256 ? kBisLevels : 1, NODES = (1 << L) - 1;
   if (a.active && !*a.active) return;  // uniform across the cluster: no barrier is skipped by a subset
   cg::cluster_group cl = cg::this_cluster();
   __shared__ double slots[3][2];
   __shared__ double wsm[66];
+  __shared__ double bslots[2][NODES];
+  __shared__ double bsm[33 * NODES];
   extern __shared__ double2 mu_cache[];  // a.cache: (eps, w) of this thread's elements, [u][thread]
   const int gt = cl.block_rank() * blockDim.x + threadIdx.x;
   const int gs = cl.num_blocks() * blockDim.x;
@@ -208,21 +258,84 @@ __global__ void __launch_bounds__(kMuThreads) k_find_mu(const MuArgs a) {
 
   double result;
   if (a.method == 0) {
+    // L levels of the bisection per pass: the counts at all 2^L - 1
+    // midpoints of the next L levels (a binary tree of intervals, each midpoint
+    // formed exactly as the one-level loop would form it) come from one cluster
+    // reduction, then the L decisions are replayed in order; same decisions and
+    // result as one level per pass, with L times fewer dependent reductions.
     const double T = a.T;
     const double span = mx - mn + 10.0 * fmax(T, 1e-6);
     double lo = mn - span, hi = mx + span;
-    const double Td = T + 1e-12;
-    for (int it = 0; it < a.maxiter; ++it) {
-      const double mid = 0.5 * (lo + hi);
-      double cnt = 0.0, dummy = 0.0;
-      visit([&](double ev, double w) { cnt += w * expit(-(ev - mid) / Td); });
-      cluster_sum2(cl, cnt, dummy, slots, wsm, parity);
+    const double Td = T + 1e-12, iTd = 1.0 / Td;
+    int it = 0;
+    bool fixed = false;
+    while (it < a.maxiter && !fixed) {
+      double nlo[NODES + 1], nhi[NODES + 1], mid[NODES + 1];
+      nlo[1] = lo;
+      nhi[1] = hi;
+#pragma unroll
+      for (int j = 1; j <= NODES; ++j) {
+        mid[j] = 0.5 * (nlo[j] + nhi[j]);
+        if (2 * j + 1 <= NODES) {
+          nlo[2 * j] = nlo[j];
+          nhi[2 * j] = mid[j];
+          nlo[2 * j + 1] = mid[j];
+          nhi[2 * j + 1] = nhi[j];
+        }
+      }
+      // exp((e - m_j) / Td) = exp((e - m_1) / Td) * exp((m_1 - m_j) / Td) where the
+      // second factor is finite and nonzero; direct exp for the other midpoints
+      // the factors are the same for every thread: lane j - 1 of each warp evaluates
+      // factor j and the warp shares them
+      double r[NODES + 1];
+      bool fac[NODES + 1];
+      {
+        const int ln = threadIdx.x & 31;
+        double zl = 0.0;
+#pragma unroll
+        for (int j = 1; j <= NODES; ++j)
+          if (ln == j - 1) zl = (mid[1] - mid[j]) * iTd;
+        const double rl = fabs(zl) < 700.0 ? exp(zl) : 0.0;
+#pragma unroll
+        for (int j = 1; j <= NODES; ++j) {
+          fac[j] = fabs((mid[1] - mid[j]) * iTd) < 700.0;
+          r[j] = __shfl_sync(0xffffffffu, rl, j - 1);
+        }
+      }
+      double cnt[NODES];
+#pragma unroll
+      for (int j = 0; j < NODES; ++j) cnt[j] = 0.0;
+      visit([&](double ev, double w) {
+        const double g = exp((ev - mid[1]) * iTd);
+#pragma unroll
+        for (int j = 1; j <= NODES; ++j) {
+          const double x = fac[j] ? g * r[j] : exp((ev - mid[j]) * iTd);
+          cnt[j - 1] += w / (1.0 + x);
+        }
+      });
+      cluster_sum_n<NODES>(cl, cnt, bslots, bsm, parity);
       parity ^= 1;
-      const double nlo = (cnt > a.target) ? lo : mid;
-      const double nhi = (cnt > a.target) ? mid : hi;
-      if (nlo == lo && nhi == hi) break;  // exact fixed point
-      lo = nlo;
-      hi = nhi;
+      int node = 1;
+#pragma unroll
+      for (int l = 0; l < L; ++l) {
+        if (fixed || it >= a.maxiter) break;
+        // node's count and midpoint by select chains (no dynamically indexed arrays)
+        double cn = 0.0, mn_ = 0.0;
+#pragma unroll
+        for (int j = 1; j <= NODES; ++j)
+          if (j == node) { cn = cnt[j - 1]; mn_ = mid[j]; }
+        const bool above = cn > a.target;
+        const double nl = above ? lo : mn_;
+        const double nh = above ? mn_ : hi;
+        if (nl == lo && nh == hi) {  // exact fixed point
+          fixed = true;
+          break;
+        }
+        lo = nl;
+        hi = nh;
+        node = 2 * node + (above ? 0 : 1);
+        ++it;
+      }
     }
     result = 0.5 * (lo + hi);
   } else {
@@ -310,29 +423,41 @@ int hf::find_mu_internal(void* stream, int dtype, int method, int nk1, int nk2, 
     else if (method == 1) maxiter = single ? 15 : 25;
     else maxiter = 25;
   }
+  const size_t n_all = (size_t)nk1 * (size_t)nk2 * (size_t)nb;
+  if (n_all > (size_t)INT_MAX) return fail(HF_ERR_UNSUPPORTED, "more than 2^31 - 1 eigenvalues");
   MuArgs a;
   a.eps = eps; a.w = weights;
-  a.n = nk1 * nk2 * nb; a.nb = nb; a.method = method; a.maxiter = maxiter;
+  a.n = (int)n_all; a.nb = nb; a.method = method; a.maxiter = maxiter;
   a.target = n_electrons; a.T = T; a.mu0 = mu0; a.out = mu_out; a.active = active;
-  // bisection (54 FP64-bound passes of an exp and a division per element): about one
-  // element per thread, so small meshes spread over several SMs; the Newton variants
-  // (3-25 passes, bound by the cluster barrier of each pass): up to four per thread
-  const int per_thread = method == 0 ? 1 : kMuCacheU;
-  int csize = (a.n + per_thread * kMuThreads - 1) / (per_thread * kMuThreads);
+  // bisection: every pass evaluates 15 midpoints per eigenvalue, so small
+  // meshes use 256-thread CTAs with one eigenvalue per thread, spread over up to 16
+  // SMs; the Newton variants (one evaluation per pass, bound by the cluster barrier
+  // of each pass): up to four per thread of 1024-thread CTAs
+  const int threads = (method == 0 && a.n <= kMuMaxCluster * 256) ? 256 : kMuThreads;
+  const int per_cta = method == 0 ? threads : kMuCacheU * kMuThreads;
+  int csize = (a.n + per_cta - 1) / per_cta;
   if (csize < 1) csize = 1;
   if (csize > kMuMaxCluster) csize = kMuMaxCluster;
-  if (csize > 8) {  // beyond the portable 8: only as large as the device can co-schedule
-    const void* fn = single ? (const void*)k_find_mu<float> : (const void*)k_find_mu<double>;
-    static int max16[2][64] = {};  // per (precision, device): 0 unknown, else the largest schedulable size
-    int dev = 0;
-    HF_CUDA(cudaGetDevice(&dev));
-    int& mc = max16[single ? 1 : 0][dev & 63];
-    if (mc == 0) {
-      mc = 8;
+  const void* fn = threads == 256 ? (single ? (const void*)k_find_mu<float, 256> : (const void*)k_find_mu<double, 256>)
+                                  : (single ? (const void*)k_find_mu<float, kMuThreads>
+                                            : (const void*)k_find_mu<double, kMuThreads>);
+  int dev = 0;
+  HF_CUDA(cudaGetDevice(&dev));
+  // per (kernel, device), set up once under a lock: the largest schedulable cluster
+  // size (beyond the portable 8 only as large as the device can co-schedule) and the
+  // opt-in for the shared-memory cache of the largest block
+  static std::mutex mu_setup;
+  static std::map<std::pair<const void*, int>, int> max_cluster;
+  {
+    std::lock_guard<std::mutex> lk(mu_setup);
+    auto key = std::make_pair(fn, dev);
+    auto it = max_cluster.find(key);
+    if (it == max_cluster.end()) {
+      int mc = 8;
       if (cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
         cudaLaunchConfig_t q = {};
         q.gridDim = dim3(kMuMaxCluster, 1, 1);
-        q.blockDim = dim3(kMuThreads, 1, 1);
+        q.blockDim = dim3(threads, 1, 1);
         cudaLaunchAttribute qa[1];
         qa[0].id = cudaLaunchAttributeClusterDimension;
         qa[0].val.clusterDim.x = kMuMaxCluster;
@@ -344,25 +469,17 @@ int hf::find_mu_internal(void* stream, int dtype, int method, int nk1, int nk2, 
         if (cudaOccupancyMaxPotentialClusterSize(&c, fn, &q) == cudaSuccess && c >= 8) mc = c < kMuMaxCluster ? c : kMuMaxCluster;
       }
       cudaGetLastError();  // a refused query leaves the portable size
+      HF_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)((size_t)kMuCacheU * kMuThreads * sizeof(double2))));
+      it = max_cluster.emplace(key, mc).first;
     }
-    if (csize > mc) csize = mc;
+    if (csize > it->second) csize = it->second;
   }
-  a.cache = a.n <= kMuCacheU * csize * kMuThreads ? 1 : 0;
-  const size_t cache_bytes = (size_t)kMuCacheU * kMuThreads * sizeof(double2);
-  if (a.cache) {
-    static bool smem_set[2][64] = {};  // per (precision, device)
-    int dev = 0;
-    HF_CUDA(cudaGetDevice(&dev));
-    bool& done = smem_set[single ? 1 : 0][dev & 63];
-    if (!done) {
-      const void* fn = single ? (const void*)k_find_mu<float> : (const void*)k_find_mu<double>;
-      HF_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cache_bytes));
-      done = true;
-    }
-  }
+  a.cache = a.n <= kMuCacheU * csize * threads ? 1 : 0;
+  const size_t cache_bytes = (size_t)kMuCacheU * threads * sizeof(double2);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(csize, 1, 1);
-  cfg.blockDim = dim3(kMuThreads, 1, 1);
+  cfg.blockDim = dim3(threads, 1, 1);
   cfg.dynamicSmemBytes = a.cache ? cache_bytes : 0;
   cfg.stream = static_cast<cudaStream_t>(stream);
   cudaLaunchAttribute attr[1];
@@ -372,7 +489,12 @@ int hf::find_mu_internal(void* stream, int dtype, int method, int nk1, int nk2, 
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  if (single) HF_CUDA(cudaLaunchKernelEx(&cfg, k_find_mu<float>, a));
-  else HF_CUDA(cudaLaunchKernelEx(&cfg, k_find_mu<double>, a));
+  if (threads == 256) {
+    if (single) HF_CUDA(cudaLaunchKernelEx(&cfg, k_find_mu<float, 256>, a));
+    else HF_CUDA(cudaLaunchKernelEx(&cfg, k_find_mu<double, 256>, a));
+  } else {
+    if (single) HF_CUDA(cudaLaunchKernelEx(&cfg, k_find_mu<float, kMuThreads>, a));
+    else HF_CUDA(cudaLaunchKernelEx(&cfg, k_find_mu<double, kMuThreads>, a));
+  }
   return HF_OK;
 }
