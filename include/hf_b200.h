@@ -238,6 +238,14 @@ int hf_density_from_Qp(void* stream, int dtype, int batch, int nb, const void* Q
 int hf_fock_orbital(void* stream, int dtype, int batch, int nb, const void* Q, const void* F,
                     void* Ft);
 int hf_eigh(void* stream, int dtype, int batch, int nb, const void* A, void* w, void* V);
+/* Extension (no counterpart in the reference): complex128 eigendecomposition of nk
+ * Hermitian nb x nb matrices (nb <= 8; A hermitised) by a lane-per-column cyclic
+ * Jacobi, eigenvalues ascending in w, eigenvectors as the columns of Qout.  With a
+ * starting basis Qin (may be NULL; may equal Qout) the rotation is applied to
+ * Qin^H A Qin and Qout = Qin V: when Qin already diagonalises a nearby matrix (the
+ * previous SCF iteration's Fock matrix), the sweeps converge at once.  The result
+ * is an exact decomposition either way (to the Jacobi tolerance). */
+int hf_eigh_warm(void* stream, int nk, int nb, const void* A, const void* Qin, void* Qout, void* w);
 int hf_cayley_retract(void* stream, int dtype, int batch, int nb, const void* d, double tau,
                       void* U);
 int hf_cayley_spectral(void* stream, int dtype, int batch, int nb, const void* d, void* V,
@@ -366,13 +374,31 @@ int hf_cg_solve(void* stream, const hf_cg_problem* problem, const hf_cg_config* 
  * fock_matrix), the per-iteration histories hist_E, hist_D, hist_C (HOST
  * float64, max_iter entries each, may be NULL) and scalars_out (HOST, 4
  * float64): energy, chemical potential, iterations, converged.  Synchronises
- * `stream` once per iteration (twice for ODA or a trust-radius clip). */
+ * `stream` once per iteration (twice for ODA or a trust-radius clip).
+ * Extensions (no counterpart in the reference; zero keeps its behaviour):
+ *  - fp32_exchange != 0: mixed precision.  Builds run the exchange FFT in FP32
+ *    (HF_FOCK_FFT_FP32) while the previous iteration's density residual exceeds
+ *    fp32_switch_density; from the first iteration below it every build is FP64,
+ *    the DIIS history restarts, and convergence is only declared on FP64 builds,
+ *    so the result is the FP64 fixed point.  scalars_out then has a fifth entry:
+ *    the first FP64 iteration (-1 if the FP32 phase never ended).
+ *  - mu_method 2: the chemical potentials come from the Newton-bracket solver
+ *    (solver.py:62-101 rules), started at mu = 0 in the first iteration and at
+ *    the previous iteration's mu afterwards, instead of the 54-step bisection
+ *    (the same root to rounding; level_shift must be 0).
+ *  - warm_eigh != 0 (nb <= 8): the eigendecompositions of the iterations after
+ *    the first start from the previous iteration's eigenvectors (hf_eigh_warm);
+ *    the same decomposition to the Jacobi tolerance, in fewer sweeps. */
 typedef struct hf_scf_config {
   int max_iter;
   double density_tol, comm_tol, mixing, level_shift;
   int acceleration; /* 0 linear, 1 diis, 2 oda */
   int diis_size, diis_start;
   double diis_damping, trust_radius;
+  int fp32_exchange;          /* extension, see above */
+  double fp32_switch_density; /* extension */
+  int mu_method;              /* extension: 0 bisection (reference), 2 Newton-bracket warm start */
+  int warm_eigh;              /* extension: eigh from the previous iteration's eigenvectors (nb <= 8) */
 } hf_scf_config;
 
 int hf_scf_workspace_size(const hf_cg_problem* problem, const hf_scf_config* config, size_t* bytes);

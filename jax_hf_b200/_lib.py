@@ -64,6 +64,7 @@ _SIGS = {
     "hf_density_from_Qp": ([vp, i32, i32, i32, vp, vp, vp], i32),
     "hf_fock_orbital": ([vp, i32, i32, i32, vp, vp, vp], i32),
     "hf_eigh": ([vp, i32, i32, i32, vp, vp, vp], i32),
+    "hf_eigh_warm": ([vp, i32, i32, vp, vp, vp, vp], i32),
     "hf_cayley_retract": ([vp, i32, i32, i32, vp, f64, vp], i32),
     "hf_cayley_spectral": ([vp, i32, i32, i32, vp, vp, vp], i32),
     "hf_cayley_unitary": ([vp, i32, i32, i32, vp, vp, f64, vp], i32),

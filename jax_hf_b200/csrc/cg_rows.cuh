@@ -580,12 +580,15 @@ __device__ __forceinline__ void jacobi_smem_cols(double2* SA, double2* SV, doubl
   }
 }
 
-// eps, Q <- eigh(A) per k (A = F0 at init; Ft = Q^H F Q at finalize, then Q <- Q V),
-// eigenvalues ascending (solver.py:389, 622-626).
+// eps, Qout <- eigh(A) per k, eigenvalues ascending (solver.py:389, 622-626).  With a
+// starting basis Qin (rotate): A is taken in that basis (Qin^H A Qin, nearly diagonal
+// when Qin already diagonalises a nearby matrix, so the sweeps converge at once) and
+// Qout = Qin V.  Qin may equal Qout: a k-point's rows are read before they are written.
 constexpr int kEigWarps = 2;
 template <int NB>
-__global__ void __launch_bounds__(32 * kEigWarps, 8) k_cgr_eig(CgArgs a, const double2* __restrict__ A, int rotate,
-                                                            double tol) {
+__device__ __forceinline__ void eig_cols(int nk, const double2* __restrict__ A, const double2* Qin, double2* Qout,
+                                         double* eps, double tol) {
+  const bool rotate = Qin != nullptr;
   using RG = RowGroup<NB>;
   constexpr int G = RG::G, KPW = RG::KPW, LP = RG::LP, MAT = RG::MAT, NP = JacobiPairs<NB>::M / 2;
   __shared__ double2 st[kEigWarps][KPW][3 * MAT + 2 * NP];
@@ -596,9 +599,9 @@ __global__ void __launch_bounds__(32 * kEigWarps, 8) k_cgr_eig(CgArgs a, const d
   double2* SV = SA + MAT;
   double2* SP = SV + MAT;
   double* SW = sw[w][g];
-  for (int kb = (blockIdx.x * kEigWarps + w) * KPW; kb < a.nk; kb += gridDim.x * kEigWarps * KPW) {
+  for (int kb = (blockIdx.x * kEigWarps + w) * KPW; kb < nk; kb += gridDim.x * kEigWarps * KPW) {
     const int k = kb + g;
-    const bool on = k < a.nk && c < NB;
+    const bool on = k < nk && c < NB;
     const size_t base = (size_t)k * NB * NB + c;
     if (on) {
 #pragma unroll
@@ -609,7 +612,7 @@ __global__ void __launch_bounds__(32 * kEigWarps, 8) k_cgr_eig(CgArgs a, const d
       if (on) {
 #pragma unroll
         for (int r = 0; r < NB; ++r) {
-          q[r] = q_cur(a)[base + (size_t)r * NB];
+          q[r] = Qin[base + (size_t)r * NB];
           SQ[r * LP + c] = q[r];
         }
       }
@@ -669,7 +672,7 @@ __global__ void __launch_bounds__(32 * kEigWarps, 8) k_cgr_eig(CgArgs a, const d
       int rk = 0;
 #pragma unroll
       for (int j = 0; j < NB; ++j) rk += (SW[j] < wc) || (SW[j] == wc && j < c);
-      a.eps[(size_t)k * NB + rk] = wc;
+      eps[(size_t)k * NB + rk] = wc;
       const size_t out = (size_t)k * NB * NB + rk;
       if (rotate) {  // (Q V)[r][rk] = sum_j Q[r][j] V[j][c]
 #pragma unroll
@@ -677,15 +680,28 @@ __global__ void __launch_bounds__(32 * kEigWarps, 8) k_cgr_eig(CgArgs a, const d
           double2 acc = make_double2(0.0, 0.0);
 #pragma unroll
           for (int j = 0; j < NB; ++j) acc = cfma(SQ[r * LP + j], SV[j * LP + c], acc);
-          a.Q[out + (size_t)r * NB] = acc;
+          Qout[out + (size_t)r * NB] = acc;
         }
       } else {
 #pragma unroll
-        for (int r = 0; r < NB; ++r) a.Q[out + (size_t)r * NB] = SV[r * LP + c];
+        for (int r = 0; r < NB; ++r) Qout[out + (size_t)r * NB] = SV[r * LP + c];
       }
     }
     __syncwarp();
   }
+}
+
+template <int NB>
+__global__ void __launch_bounds__(32 * kEigWarps, 8) k_cgr_eig(CgArgs a, const double2* __restrict__ A, int rotate,
+                                                            double tol) {
+  eig_cols<NB>(a.nk, A, rotate ? q_cur(a) : nullptr, a.Q, a.eps, tol);
+}
+// Standalone eigensolve: eps, Qout <- eigh(A) (Qin == nullptr) or with the starting basis Qin.
+template <int NB>
+__global__ void __launch_bounds__(32 * kEigWarps, 8) k_eig_cols(int nk, const double2* __restrict__ A,
+                                                             const double2* Qin, double2* Qout, double* eps,
+                                                             double tol) {
+  eig_cols<NB>(nk, A, Qin, Qout, eps, tol);
 }
 
 }  // namespace hf

@@ -27,28 +27,22 @@ __device__ __forceinline__ void write_partials(KSum (&acc)[NS], double* part, do
   }
 }
 
-__global__ void k_sum_partials(const double* __restrict__ part, int nblk, int ns, double* __restrict__ out) {
-  const int q = threadIdx.x;
-  if (q >= ns) return;
+// Finish of the device reductions: sum q of ns gets one CTA, whose threads take the
+// block partials (Neumaier pairs) b = t, t + blockDim, ... and merge them with the
+// fixed-shape block reduction, so the result is deterministic for a launch shape.
+// (One warp walking every partial in one dependent chain took ~150 us at 592 blocks.)
+constexpr int kSumThreads = 128;
+__global__ void __launch_bounds__(kSumThreads) k_sum_partials(const double* __restrict__ part, int nblk, int ns,
+                                                              double* __restrict__ out) {
+  __shared__ double sm[2 * 32];
+  const int q = blockIdx.x;
   KSum t;
-  // block order as before; the loads of a batch are issued before its compensated adds
-  constexpr int U = 8;
-  for (int b0 = 0; b0 < nblk; b0 += U) {
-    double v[2 * U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const bool in = b0 + u < nblk;
-      v[2 * u] = in ? part[((size_t)(b0 + u) * ns + q) * 2] : 0.0;
-      v[2 * u + 1] = in ? part[((size_t)(b0 + u) * ns + q) * 2 + 1] : 0.0;
-    }
-#pragma unroll
-    for (int u = 0; u < U; ++u)
-      if (b0 + u < nblk) {
-        t.add(v[2 * u]);
-        t.add(v[2 * u + 1]);
-      }
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
+    t.add(part[((size_t)b * ns + q) * 2]);
+    t.add(part[((size_t)b * ns + q) * 2 + 1]);
   }
-  out[q] = t.value();
+  t = block_reduce(t, sm);
+  if (threadIdx.x == 0) out[q] = t.value();
 }
 
 static int nblocks(size_t n) {
@@ -124,7 +118,11 @@ __global__ void k_gram(size_t stride, size_t len, int nb2, const double2* __rest
                        const double* __restrict__ w, double* part) {
   __shared__ double red[64];
   constexpr int np = N * (N + 1) / 2;
-  KSum acc[np];
+  // a thread sums its few elements in plain FP64; the thread, block and grid partials
+  // are then merged with compensated (Neumaier) sums
+  double acc[np];
+#pragma unroll
+  for (int q = 0; q < np; ++q) acc[q] = 0.0;
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < len; e += (size_t)gridDim.x * blockDim.x) {
     const double wk = w[e / nb2];
     double2 r[N];
@@ -134,11 +132,13 @@ __global__ void k_gram(size_t stride, size_t len, int nb2, const double2* __rest
 #pragma unroll
     for (int i = 0; i < N; ++i)
 #pragma unroll
-      for (int j = i; j < N; ++j, ++q) acc[q].add(wk * (r[i].x * r[j].x + r[i].y * r[j].y));
+      for (int j = i; j < N; ++j, ++q) acc[q] = fma(wk, fma(r[i].x, r[j].x, r[i].y * r[j].y), acc[q]);
   }
 #pragma unroll
   for (int q = 0; q < np; ++q) {
-    KSum rr = block_reduce(acc[q], red);
+    KSum t;
+    t.add(acc[q]);
+    KSum rr = block_reduce(t, red);
     if (threadIdx.x == 0) {
       part[((size_t)blockIdx.x * np + q) * 2] = rr.s;
       part[((size_t)blockIdx.x * np + q) * 2 + 1] = rr.c;
@@ -399,7 +399,7 @@ static int perk_grid(int nk) {
 
 static int finish(cudaStream_t s, double* part, int nblk, int ns, double* out) {
   HF_LAUNCH_CHECK("reduction kernel");
-  k_sum_partials<<<1, 32, 0, s>>>(part, nblk, ns, out);
+  k_sum_partials<<<ns, kSumThreads, 0, s>>>(part, nblk, ns, out);
   HF_LAUNCH_CHECK("k_sum_partials");
   return HF_OK;
 }

@@ -104,8 +104,12 @@ struct Scf {
   int herm_axpby(double a, const void* x, double b, const void* y, void* out) {
     return hf_axpby(s, (size_t)nk, nb, a, x, b, y, 1, out);
   }
+  bool fp32 = false;    // this build runs the exchange FFT in FP32
+  bool mu_warm = false;  // mu from the Newton-bracket solver started at the previous mu
+  bool eig_warm = false; // eigh started from the eigenvectors in kV (the previous decomposition)
   int fock(const void* P, void* Sg, void* H, void* F) {
-    return hf_fock_build(s, HF_C128, pb->fock_flags, pb->nk1, pb->nk2, nb, P, pb->h, pb->VR, pb->refP, pb->HH,
+    const unsigned flags = pb->fock_flags | (fp32 ? HF_FOCK_FFT_FP32 : 0u);
+    return hf_fock_build(s, HF_C128, flags, pb->nk1, pb->nk2, nb, P, pb->h, pb->VR, pb->refP, pb->HH,
                          pb->w2d, pb->n_contact, pb->contact_g, pb->contact_Oi, pb->contact_Oj, Sg, H, F,
                          at<void>(kFOCKWS), fock_ws);
   }
@@ -117,9 +121,15 @@ struct Scf {
   int density_from_fock(const void* F, void* P_out) {
     int st;
     double* sc = scal();
-    if ((st = hf_eigh(s, HF_C128, nk, nb, F, at<double>(kEV), at<void>(kV)))) return st;
-    if ((st = hf_find_mu(s, HF_C128, 0, nk, 1, nb, at<double>(kEV), pb->w2d, pb->n_electrons, pb->T, 0, nullptr,
-                         sc + kSMuRaw)))
+    if (eig_warm) {
+      if ((st = hf_eigh_warm(s, nk, nb, F, at<void>(kV), at<void>(kV), at<double>(kEV)))) return st;
+    } else if ((st = hf_eigh(s, HF_C128, nk, nb, F, at<double>(kEV), at<void>(kV)))) {
+      return st;
+    }
+    // mu_method 2: Newton-bracket solver, from mu = 0 in the first call and from the previous
+    // mu afterwards (the warm start reads that word before the kernel overwrites it)
+    if ((st = hf_find_mu(s, HF_C128, cf->mu_method == 2 ? 2 : 0, nk, 1, nb, at<double>(kEV), pb->w2d,
+                         pb->n_electrons, pb->T, 0, mu_warm ? sc + kSMuRaw : nullptr, sc + kSMuRaw)))
       return st;
     const double* shifted = at<double>(kEV);
     const double* mu = sc + kSMuRaw;
@@ -167,6 +177,11 @@ static int scf_check(const hf_cg_problem* pb, const hf_scf_config* cf) {
     return fail(HF_ERR_INVALID, "SCFConfig.acceleration must be 'linear', 'diis', or 'oda'");
   if (cf->diis_size <= 0) return fail(HF_ERR_INVALID, "diis_size must be positive");
   if (cf->acceleration == 1 && cf->diis_size > 16) return fail(HF_ERR_UNSUPPORTED, "hf_scf: diis_size > 16");
+  if (cf->mu_method != 0 && cf->mu_method != 2) return fail(HF_ERR_INVALID, "hf_scf: mu_method must be 0 or 2");
+  if (cf->mu_method == 2 && cf->level_shift != 0.0)
+    return fail(HF_ERR_INVALID, "hf_scf: mu_method 2 needs level_shift = 0");
+  if (cf->fp32_exchange && !(pb->fock_flags & HF_FOCK_EXCHANGE))
+    return fail(HF_ERR_INVALID, "hf_scf: fp32_exchange needs the exchange term");
   return HF_OK;
 }
 
@@ -224,17 +239,31 @@ extern "C" int hf_scf_solve(void* stream, const hf_cg_problem* pb, const hf_scf_
     HF_CUDA(cudaMemsetAsync(S.at<void>(kFHIST), 0, (size_t)nh * qbytes, s));
   }
   std::vector<double> hv(kSCoeff + 8, 0.0);
-  int k = 0;
+  int k = 0, base = 0, switch_iter = -1;  // base: first iteration of the current DIIS history
   bool converged = false;
+  double d_prev = INFINITY;
+  S.fp32 = cf->fp32_exchange != 0;
   while (k < cf->max_iter && !converged) {
     void* F = S.at<void>(kF);
     void* Pn = S.at<void>(kPN);
+    if (S.fp32 && d_prev <= cf->fp32_switch_density) {  // FP64 from here on, with a fresh DIIS history
+      S.fp32 = false;
+      switch_iter = k;
+      base = k;
+      if (diis) {
+        HF_CUDA(cudaMemsetAsync(S.at<void>(kRH), 0, (size_t)nh * qbytes, s));
+        HF_CUDA(cudaMemsetAsync(S.at<void>(kFHIST), 0, (size_t)nh * qbytes, s));
+      }
+    }
+    S.mu_warm = cf->mu_method == 2 && k > 0;
+    S.eig_warm = cf->warm_eigh != 0 && nb <= 8 && k > 0;
     if ((st = S.build_and_occupy(density, F, Pn))) return st;
-    void* R_out = diis ? (void*)(S.at<unsigned char>(kRH) + (size_t)(k % nh) * qbytes) : (void*)S.at<void>(kRH);
+    const int kd = k - base;  // index in the current DIIS history
+    void* R_out = diis ? (void*)(S.at<unsigned char>(kRH) + (size_t)(kd % nh) * qbytes) : (void*)S.at<void>(kRH);
     if ((st = hf_scf_residuals(s, nk, nb, F, density, Pn, w2d, R_out, S.at<void>(kDELTA), sc + kSSums, ops)))
       return st;
     if (diis) {
-      HF_CUDA(cudaMemcpyAsync(S.at<unsigned char>(kFHIST) + (size_t)(k % nh) * qbytes, F, qbytes,
+      HF_CUDA(cudaMemcpyAsync(S.at<unsigned char>(kFHIST) + (size_t)(kd % nh) * qbytes, F, qbytes,
                               cudaMemcpyDeviceToDevice, s));
       if (nh <= 6) {
         if ((st = hf_gram(s, nh, nq, nk, nb, S.at<void>(kRH), w2d, sc + kSGram, ops))) return st;
@@ -243,7 +272,8 @@ extern "C" int hf_scf_solve(void* stream, const hf_cg_problem* pb, const hf_scf_
     if ((st = S.read(hv.data(), sc, kSCoeff))) return st;
     const double E_host = hv[kSE];
     const double d_res = std::sqrt(hv[kSSums] / wsum), c_res = std::sqrt(hv[kSSums + 1] / wsum);
-    converged = d_res <= cf->density_tol && c_res <= cf->comm_tol;
+    converged = !S.fp32 && d_res <= cf->density_tol && c_res <= cf->comm_tol;
+    d_prev = d_res;
     void* updated = S.at<void>(kUPD);
     if (diis) {
       // B_ij = sum_k w Re tr(R_i^H R_j) over every history slot (zeros where unused)
@@ -267,7 +297,7 @@ extern "C" int hf_scf_solve(void* stream, const hf_cg_problem* pb, const hf_scf_
       double bmax = 0.0;
       for (double v : B) bmax = std::fmax(bmax, std::fabs(v));
       bmax = std::fmax(bmax, 1e-30);
-      const int count = k + 1 < nh ? k + 1 : nh;
+      const int count = kd + 1 < nh ? kd + 1 : nh;
       const int m = nh + 1;
       std::vector<double> A((size_t)m * m, 0.0), rhs(m, 0.0), sol;
       for (int i = 0; i < nh; ++i) {
@@ -330,7 +360,10 @@ extern "C" int hf_scf_solve(void* stream, const hf_cg_problem* pb, const hf_scf_
     if (hist_C) hist_C[k] = c_res;
     ++k;
   }
-  // final build at the returned density (reference_scf.py:345-347)
+  // final build at the returned density (reference_scf.py:345-347), FP64 in every mode
+  S.fp32 = false;
+  S.mu_warm = cf->mu_method == 2 && k > 0;
+  S.eig_warm = cf->warm_eigh != 0 && nb <= 8 && k > 0;
   if ((st = S.build_and_occupy(density, fock, S.at<void>(kPN)))) return st;
   double fin[3] = {0.0, 0.0, 0.0};
   if ((st = S.read(fin, sc, 3))) return st;
@@ -338,5 +371,6 @@ extern "C" int hf_scf_solve(void* stream, const hf_cg_problem* pb, const hf_scf_
   scalars_out[1] = fin[kSMu];
   scalars_out[2] = (double)k;
   scalars_out[3] = converged ? 1.0 : 0.0;
+  if (cf->fp32_exchange) scalars_out[4] = (double)switch_iter;
   return HF_OK;
 }

@@ -843,6 +843,17 @@ static int cg_eig(CgRun& r, cudaStream_t s, const double2* A, int rotate) {
   return HF_OK;
 }
 
+template <int NB>
+static int eig_cols_launch(cudaStream_t s, int nk, const double2* A, const double2* Qin, double2* Qout,
+                           double* eps) {
+  const int per_block = kEigWarps * RowGroup<NB>::KPW;
+  int b = (nk + per_block - 1) / per_block;
+  if (b > 148 * 32) b = 148 * 32;
+  k_eig_cols<NB><<<b < 1 ? 1 : b, 32 * kEigWarps, 0, s>>>(nk, A, Qin, Qout, eps, kEigTol);
+  HF_LAUNCH_CHECK("k_eig_cols");
+  return HF_OK;
+}
+
 static int cg_iteration_warp(CgRun& r, cudaStream_t s, const hf_cg_config& cf, bool fp32);
 
 static int cg_iteration(CgRun& r, cudaStream_t s, const hf_cg_config& cf, bool fp32) {
@@ -1313,4 +1324,23 @@ extern "C" int hf_cg_solve_batch(void* stream, const hf_cg_batch_item* items, in
   st = run();
   cleanup();
   return st;
+}
+
+// Eigendecomposition of nk Hermitian nb x nb matrices (nb <= 8) by the lane-per-column
+// cyclic Jacobi of the CG driver, optionally from a starting basis (see the header).
+extern "C" int hf_eigh_warm(void* stream, int nk, int nb, const void* A, const void* Qin, void* Qout, void* eps) {
+  if (nk < 1 || nb < 1 || nb > 8) return fail(HF_ERR_UNSUPPORTED, "hf_eigh_warm: needs nk >= 1 and 1 <= nb <= 8");
+  if (!A || !Qout || !eps) return fail(HF_ERR_INVALID, "hf_eigh_warm: NULL argument");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const double2* a = static_cast<const double2*>(A);
+  const double2* qi = static_cast<const double2*>(Qin);
+  double2* qo = static_cast<double2*>(Qout);
+  double* e = static_cast<double*>(eps);
+  switch (nb) {
+#define HF_NB_CASE(N) case N: return eig_cols_launch<N>(s, nk, a, qi, qo, e);
+    HF_NB_CASE(1) HF_NB_CASE(2) HF_NB_CASE(3) HF_NB_CASE(4) HF_NB_CASE(5) HF_NB_CASE(6) HF_NB_CASE(7) HF_NB_CASE(8)
+#undef HF_NB_CASE
+    default: break;
+  }
+  return fail(HF_ERR_UNSUPPORTED, "hf_eigh_warm: nb > 8");
 }

@@ -48,6 +48,16 @@ class SCFConfig:
     diis_damping: float = 1.0
     trust_radius: float = 0.0
     project_fn: Callable[[Any], Any] | None = None
+    # extensions (the library's SCF driver only; defaults keep the reference behaviour):
+    # fp32_exchange runs the exchange FFT in FP32 while the density residual is above
+    # fp32_switch_density, then FP64 to convergence (the FP64 fixed point);
+    # mu_method="newton" takes each iteration's mu from the Newton-bracket solver
+    # started at the previous mu instead of the 54-step bisection (same root to rounding);
+    # warm_eigh starts each eigendecomposition (nb <= 8) from the previous eigenvectors
+    fp32_exchange: bool = False
+    fp32_switch_density: float = 1e-5
+    mu_method: str = "bisection"
+    warm_eigh: bool = False
 
     def __post_init__(self) -> None:
         if self.max_iter <= 0:
@@ -57,6 +67,8 @@ class SCFConfig:
                              f"got {self.acceleration!r}")
         if self.diis_size <= 0:
             raise ValueError("diis_size must be positive")
+        if self.mu_method not in ("bisection", "newton"):
+            raise ValueError(f"SCFConfig.mu_method must be 'bisection' or 'newton'; got {self.mu_method!r}")
 
 
 @dataclass(frozen=True)
@@ -122,6 +134,9 @@ def solve_scf(kernel, P0, n_electrons: float, *, config: SCFConfig | None = None
     validate_electron_count(w2d, nb, n_electrons, context="n_electrons")
     if USE_NATIVE and fock_build_fn is None and project is None and (cfg.acceleration != "diis" or cfg.diis_size <= 16):
         return _solve_scf_native(kernel, P0, n_electrons, cfg)
+    if cfg.fp32_exchange or cfg.mu_method != "bisection" or cfg.warm_eigh:
+        raise ValueError("SCFConfig.fp32_exchange, mu_method='newton' and warm_eigh run in the library's SCF driver, "
+                         "which takes no project_fn or fock_build_fn.")
     a = kernel.as_args()
     VR = a["VR"] if kernel.dtype == cd else (a["VR"].to(cd) if a["VR"].is_complex() else a["VR"].to(torch.float64))
     fock_kw = dict(h=h, VR=VR, refP=kernel.refP if kernel.dtype == cd else kernel.refP.to(cd), HH=kernel.HH.double(),
@@ -272,7 +287,8 @@ class _ScfConfig(C.Structure):
     _fields_ = [("max_iter", C.c_int), ("density_tol", C.c_double), ("comm_tol", C.c_double),
                 ("mixing", C.c_double), ("level_shift", C.c_double), ("acceleration", C.c_int),
                 ("diis_size", C.c_int), ("diis_start", C.c_int), ("diis_damping", C.c_double),
-                ("trust_radius", C.c_double)]
+                ("trust_radius", C.c_double), ("fp32_exchange", C.c_int), ("fp32_switch_density", C.c_double),
+                ("mu_method", C.c_int), ("warm_eigh", C.c_int)]
 
 
 def _solve_scf_native(kernel, P0, n_electrons, cfg):
@@ -296,7 +312,8 @@ def _solve_scf_native(kernel, P0, n_electrons, cfg):
     acc = {"linear": 0, "diis": 1, "oda": 2}[cfg.acceleration]
     sc = _ScfConfig(int(cfg.max_iter), float(cfg.density_tol), float(cfg.comm_tol), float(cfg.mixing),
                     float(cfg.level_shift), acc, int(cfg.diis_size), int(cfg.diis_start), float(cfg.diis_damping),
-                    float(cfg.trust_radius))
+                    float(cfg.trust_radius), int(bool(cfg.fp32_exchange)), float(cfg.fp32_switch_density),
+                    2 if cfg.mu_method == "newton" else 0, int(bool(cfg.warm_eigh)))
     need = C.c_size_t(0)
     _lib.check(L.hf_scf_workspace_size(C.byref(pb), C.byref(sc), C.byref(need)))
     ws = _lib.workspace(need.value, dev, "scf")
@@ -305,7 +322,7 @@ def _solve_scf_native(kernel, P0, n_electrons, cfg):
     fock = torch.empty_like(P0d)
     m = int(cfg.max_iter)
     hist = np.zeros((3, m))
-    out = np.zeros(4)
+    out = np.full(5, -1.0)
     dp = lambda a: a.ctypes.data_as(C.c_void_p)
     _lib.check(L.hf_scf_solve(_lib.stream_ptr(dev), C.byref(pb), C.byref(sc), P0d.data_ptr(), density.data_ptr(),
                               fock.data_ptr(), dp(hist[0]), dp(hist[1]), dp(hist[2]), dp(out), ws.data_ptr(),
@@ -324,7 +341,65 @@ def _solve_scf_native(kernel, P0, n_electrons, cfg):
                      energy=torch.tensor(float(out[0]), dtype=torch.float64, device=dev),
                      chemical_potential=torch.tensor(float(out[1]), dtype=torch.float64, device=dev),
                      iterations=n_iter, converged=converged, message=message,
-                     history={"E": hE, "density_residual": hD, "commutator_residual": hC})
+                     history={"E": hE, "density_residual": hD, "commutator_residual": hC,
+                              "fp32_switch_iter": int(out[4]) if cfg.fp32_exchange else -1})
+
+
+def solve_scf_batch(kernels, P0s, n_electrons, *, config: SCFConfig | None = None, workers: int = 16,
+                    return_times: bool = False):
+    """Many independent SCF solves at once (extension; density scans).
+
+    Each solve has the semantics of ``solve_scf(kernel, P0, n, config=config)``
+    through the library's SCF driver.  ``workers`` host threads each own a CUDA
+    stream and take the next solve (longest first, by nk1 nk2 nb^2) until none
+    is left; the driver's once-per-iteration scalar read blocks only its own
+    thread, so the solves of the other streams keep the GPU busy.  Returns the
+    list of ``SCFResult`` (and, with ``return_times``, each solve's wall time
+    in ms, from its start on its stream to its final scalars).
+    """
+    import threading
+    import time
+    cfg = config or SCFConfig()
+    n = len(kernels)
+    if n == 0 or len(P0s) != n or len(n_electrons) != n:
+        raise ValueError("kernels, P0s and n_electrons must be non-empty and of equal length.")
+    if cfg.project_fn is not None:
+        raise ValueError("solve_scf_batch takes no project_fn.")
+    dev = kernels[0].device
+    order = sorted(range(n), key=lambda i: -int(np.prod(kernels[i].shape)) * int(kernels[i].shape[-1]))
+    nxt = iter(order)
+    lock = threading.Lock()
+    results, times, errors = [None] * n, [0.0] * n, []
+    main = torch.cuda.current_stream(dev)
+    ready = torch.cuda.Event()
+    ready.record(main)
+    streams = [torch.cuda.Stream(dev) for _ in range(max(1, min(int(workers), n)))]
+
+    def work(stream):
+        try:
+            stream.wait_event(ready)
+            with torch.cuda.device(dev), torch.cuda.stream(stream):
+                while True:
+                    with lock:
+                        i = next(nxt, None)
+                    if i is None or errors:
+                        return
+                    t0 = time.perf_counter()
+                    results[i] = solve_scf(kernels[i], P0s[i], n_electrons[i], config=cfg)
+                    times[i] = 1e3 * (time.perf_counter() - t0)
+        except Exception as exc:  # re-raised on the calling thread
+            errors.append(exc)
+
+    threads = [threading.Thread(target=work, args=(st,)) for st in streams]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    for st in streams:
+        main.wait_stream(st)
+    if errors:
+        raise errors[0]
+    return (results, times) if return_times else results
 
 
 def _linear(ops, density, delta, mixing, project, proj_herm):

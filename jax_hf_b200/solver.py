@@ -51,6 +51,16 @@ class SolverConfig:
     fp32_exchange: bool = False
     fp32_switch_rel: float = 3e-7
     chunk: int = 4
+    # polish="scf": after the CG loop, an FP64 SCF-DIIS run from its density to the
+    # self-consistent fixed point (density residual <= polish_density_tol); the CG's
+    # plateau stop ends 1e-9 .. 1e-6 (relative) above that point in energy
+    polish: str = "none"
+    polish_density_tol: float = 1e-8
+    polish_comm_tol: float = 1e-7
+    polish_max_iter: int = 100
+    # an FP64 reference solution (energy, and optionally density) to report errors against
+    reference_energy: float | None = None
+    reference_density: Any = None
 
 
 class SolveResult(NamedTuple):
@@ -249,7 +259,51 @@ def _solve_cg(kernel, P0, n_electrons, cfg: SolverConfig, fock_build_fn=None):
                       energy=sc[1].clone(), n_iter=torch.tensor(int(s[2]), dtype=torch.int32),
                       converged=torch.tensor(bool(s[3])), history=hist)
     res.history["fp32_switch_iter"] = int(s[5])
+    return _finish(kernel, res, n_electrons, cfg)
+
+
+def _polish(kernel, res: SolveResult, n_electrons, cfg: SolverConfig) -> SolveResult:
+    """FP64 SCF-DIIS from the CG density to the fixed point (the library's SCF driver, Newton
+    mu warm-started from the previous iteration); orbitals and occupations from eigh(F)."""
+    from .reference_scf import SCFConfig, solve_scf
+    r = solve_scf(kernel, res.density, n_electrons,
+                  config=SCFConfig(acceleration="diis", density_tol=float(cfg.polish_density_tol),
+                                   comm_tol=float(cfg.polish_comm_tol), max_iter=int(cfg.polish_max_iter),
+                                   mu_method="newton", warm_eigh=True))
+    return _from_scf(kernel, r, res.n_iter, res.history, float(res.energy))
+
+
+def _from_scf(kernel, r, n_iter, history, cg_energy):
+    from .linalg import eigh
+    eps, Q = eigh(r.fock_matrix)
+    T = max(float(kernel.T), 1e-12)
+    mu = torch.as_tensor(r.chemical_potential, dtype=torch.float64, device=eps.device)
+    p = torch.sigmoid((mu - eps.to(torch.float64)) / T)
+    hist = dict(history)
+    hist.update(polish_iterations=int(r.iterations), polish_converged=bool(r.converged), cg_energy=cg_energy)
+    return SolveResult(Q=Q.to(kernel.dtype), p=p.to(kernel.real_dtype), mu=mu.to(kernel.real_dtype),
+                       density=r.density_matrix.to(kernel.dtype), fock=r.fock_matrix.to(kernel.dtype),
+                       energy=torch.as_tensor(r.energy, dtype=torch.float64), n_iter=n_iter,
+                       converged=torch.tensor(bool(r.converged)), history=hist)
+
+
+def _report(res: SolveResult, cfg: SolverConfig) -> SolveResult:
+    """Errors against a supplied FP64 reference solution, in the history."""
+    if cfg.reference_energy is not None:
+        Eref = float(cfg.reference_energy)
+        res.history["rel_dE_vs_reference"] = abs(float(res.energy) - Eref) / max(abs(Eref), 1e-300)
+    if cfg.reference_density is not None:
+        D = torch.as_tensor(cfg.reference_density).to(res.density.device, res.density.dtype)
+        res.history["max_abs_dP_vs_reference"] = float((res.density - D).abs().max())
     return res
+
+
+def _finish(kernel, res, n_electrons, cfg):
+    if str(cfg.polish).lower() == "scf":
+        res = _polish(kernel, res, n_electrons, cfg)
+    elif str(cfg.polish).lower() != "none":
+        raise ValueError(f"SolverConfig.polish must be 'none' or 'scf'; got {cfg.polish!r}")
+    return _report(res, cfg)
 
 
 def solve_direct_minimization(kernel, P0, n_electrons: float, *, config: SolverConfig | None = None,
@@ -376,4 +430,19 @@ def solve_batch(kernels, P0s, n_electrons, *, config: SolverConfig | None = None
                                    n_iter=torch.tensor(int(s[2]), dtype=torch.int32),
                                    converged=torch.tensor(bool(s[3])), history=hist))
     del keep
-    return (results, list(times)) if return_times else results
+    times = list(times)
+    if str(cfg.polish).lower() == "scf":
+        # the FP64 polish of every solve, on concurrent streams (one host thread each)
+        import time as _time
+        from .reference_scf import SCFConfig, solve_scf_batch
+        t0 = _time.perf_counter()
+        pol = solve_scf_batch(kernels, [r.density for r in results], list(n_electrons),
+                              config=SCFConfig(acceleration="diis", density_tol=float(cfg.polish_density_tol),
+                                               comm_tol=float(cfg.polish_comm_tol),
+                                               max_iter=int(cfg.polish_max_iter), mu_method="newton",
+                                               warm_eigh=True),
+                              workers=lanes, return_times=True)
+        results = [_from_scf(k, r, res.n_iter, res.history, float(res.energy))
+                   for k, r, res in zip(kernels, pol[0], results)]
+        times = [a + b for a, b in zip(times, pol[1])]
+    return (results, times) if return_times else results
