@@ -291,21 +291,31 @@ def run_ours(args, ws, rank, local):
 
 
 def run_solves(dev):
-    """Whole-solve throughput on the solver workloads (device time, CUDA events).
+    """Whole-solve throughput on the solver workloads (device time, CUDA events) and the
+    error of every solve against the FP64 oracle.
 
-    scf_diis_24x24_nb4: solve_scf (DIIS), FP64.  cg_144x144_nb8: CG at tol_E=1e-9,
-    plain FP64 against mixed (FP32 exchange, FP64 finish).  density_scan_64: the 64
-    solves of the scan (meshes 36..120, nb 4/6/8, CG tol_E=1e-9) solve by solve in
-    FP64, then batched (one native call, 16 streams) in FP64 and mixed; |dE/E| of
-    every batched solve against the same solve's plain FP64 result.
+    The FP64 oracle energy is the self-consistent fixed point computed by the CPU oracle
+    (tests/golden/scan64_oracle.json, tests/golden/baseline_oracle.json); the reference
+    CG's plateau stop ends 1e-9 .. 4e-6 above it, which the lines report as
+    rel_dE_vs_oracle_fixed_point next to the agreement with the oracle's own CG result.
+
+    scf_diis_24x24_nb4: solve_scf (DIIS), FP64.  cg_144x144_nb8: CG at tol_E=1e-9 in
+    FP64 (the reference algorithm) against the mixed solve (FP32-exchange CG to a coarse
+    plateau, then the FP64 SCF-DIIS polish to the fixed point).  density_scan_64: the 64
+    solves of the scan (meshes 36..120, nb 4/6/8): the reference CG solve by solve and
+    batched, the FP64 SCF-DIIS with the reference's steps solve by solve (the plain FP64
+    path that reaches |dE/E| <= 1e-9), and the mixed solvers batched.
     """
     import torch
     import jax_hf_b200 as G
     from jax_hf_b200 import synthetic as S
-    from jax_hf_b200.reference_scf import SCFConfig, solve_scf
+    from jax_hf_b200.reference_scf import SCFConfig, solve_scf, solve_scf_batch
     from jax_hf_b200.solver import SolverConfig, solve, solve_batch
 
     stream = torch.cuda.current_stream()
+    gold = ROOT / "tests" / "golden"
+    base = json.loads((gold / "baseline_oracle.json").read_text())
+    fx = json.loads((gold / "scan64_oracle.json").read_text())["rows"]
 
     def ev_time(fn, reps=1):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -320,8 +330,7 @@ def run_solves(dev):
 
     def median_run(fn, n):
         # median time of n calls; only the last result is kept, so the caching allocator can reuse
-        # the previous call's output blocks (holding every result would force fresh device
-        # allocations inside the timed calls)
+        # the previous call's output blocks
         ts, res = [], None
         for _ in range(n):
             res = None
@@ -329,72 +338,107 @@ def run_solves(dev):
             ts.append(t)
         return res, float(statistics.median(ts))
 
+    def rel(E, Eo):
+        return abs(float(E) - Eo) / abs(Eo)
+
     out = {}
-    # SCF-DIIS 24x24 nb=4
+    # SCF-DIIS 24x24 nb=4 (reference steps)
     p0 = S.scf_diis_24()
     K0 = G.HartreeFockKernel(**p0.kernel_kwargs())
     P00 = torch.zeros((24, 24, 4, 4), dtype=torch.complex128, device=dev)
     scfg = SCFConfig(acceleration="diis")
-    for _ in range(3):  # first calls load kernels and capture / instantiate graphs
+    for _ in range(3):  # first calls load kernels
         solve_scf(K0, P00, p0.n_electrons, config=scfg)
     r0, ms0 = median_run(lambda: solve_scf(K0, P00, p0.n_electrons, config=scfg), 7)
-    out["scf_diis_24x24_nb4_fp64"] = {"solves_per_s": round(1e3 / ms0, 2), "ms_per_solve": round(ms0, 2),
-                                     "iterations": int(r0.iterations), "converged": bool(r0.converged),
-                                     "energy": float(r0.energy)}
-    # CG 144x144 nb=8, FP64 vs mixed
+    o0 = base["scf_diis_24x24_nb4"]
+    out["scf_diis_24x24_nb4_fp64"] = {
+        "solves_per_s": round(1e3 / ms0, 2), "ms_per_solve": round(ms0, 2), "iterations": int(r0.iterations),
+        "converged": bool(r0.converged), "energy": float(r0.energy),
+        "rel_dE_vs_oracle_same_algorithm": rel(r0.energy, o0["reference_algorithm"]["energy"]),
+        "rel_dE_vs_oracle_fixed_point": rel(r0.energy, o0["fixed_point_energy"])}
+    # CG 144x144 nb=8: FP64 reference algorithm vs the mixed solve
     p2 = S.cg_144()
     K2 = G.HartreeFockKernel(**p2.kernel_kwargs())
     P02 = torch.zeros((144, 144, 8, 8), dtype=torch.complex128, device=dev)
-    res = {}
-    for name, cfg in (("fp64", SolverConfig(max_iter=400, tol_E=1e-9)),
-                      ("mixed", SolverConfig(max_iter=400, tol_E=1e-9, fp32_exchange=True))):
-        for _ in range(3):  # first calls load kernels and capture / instantiate graphs
+    o2 = base["cg_144x144_nb8"]
+    cfgs = (("fp64", SolverConfig(max_iter=400, tol_E=1e-9)),
+            ("mixed", SolverConfig(max_iter=400, tol_E=1e-6, fp32_exchange=True, fp32_switch_rel=1e-6,
+                                   polish="scf")))
+    cg2 = {}
+    for name, cfg in cfgs:
+        for _ in range(3):
             solve(K2, P02, p2.n_electrons, config=cfg)
         r, ms = median_run(lambda: solve(K2, P02, p2.n_electrons, config=cfg), 7)
-        res[name] = (r, ms)
-    E64 = float(res["fp64"][0].energy)
-    cg2 = {}
-    for name, (r, ms) in res.items():
         cg2[name] = {"solves_per_s": round(1e3 / ms, 2), "ms_per_solve": round(ms, 2), "n_iter": int(r.n_iter),
                      "converged": bool(r.converged), "energy": float(r.energy),
-                     "rel_dE_vs_fp64": abs(float(r.energy) - E64) / abs(E64),
-                     "max_abs_dP_vs_fp64": float((r.density - res["fp64"][0].density).abs().max())}
+                     "rel_dE_vs_oracle_fixed_point": rel(r.energy, o2["fixed_point_energy"]),
+                     "rel_dE_vs_oracle_reference_cg": rel(r.energy, o2["reference_algorithm"]["energy"])}
+        if name == "mixed":
+            cg2[name]["polish_iterations"] = int(r.history["polish_iterations"])
     out["cg_144x144_nb8"] = cg2
     # density scan: 64 solves
     probs = S.density_scan(64)
     Ks = [G.HartreeFockKernel(**p.kernel_kwargs()) for p in probs]
     P0s = [torch.zeros((p.nk, p.nk, p.nb, p.nb), dtype=torch.complex128, device=dev) for p in probs]
     nes = [p.n_electrons for p in probs]
+    Efp = np.array([r["energy"] for r in fx])
+    Ecg = np.array([r["cg_energy"] for r in fx])
     c64 = SolverConfig(max_iter=400, tol_E=1e-9)
-    cmx = SolverConfig(max_iter=400, tol_E=1e-9, fp32_exchange=True)
+    ref_scf = SCFConfig(acceleration="diis", density_tol=1e-8, comm_tol=1e-7, max_iter=300)
+    fast = dict(acceleration="diis", density_tol=1e-8, comm_tol=1e-7, max_iter=300, mu_method="newton",
+                warm_eigh=True)
+    mixed_scf = SCFConfig(**fast, fp32_exchange=True)
+    mixed_cg = SolverConfig(max_iter=400, tol_E=1e-6, fp32_exchange=True, fp32_switch_rel=1e-6, polish="scf")
+
+    def errors(Es):
+        r_fp = np.abs(np.asarray(Es) - Efp) / np.abs(Efp)
+        return {"max_rel_dE_vs_oracle_fixed_point": float(r_fp.max()),
+                "n_rel_dE_above_1e-9": int((r_fp > 1e-9).sum())}
+
+    def one_by_one(fn):
+        ts, Es = [], []
+        for K, P0, ne in zip(Ks, P0s, nes):
+            r, ms = ev_time(lambda: fn(K, P0, ne))
+            ts.append(ms)
+            Es.append(float(r.energy))
+        return ts, Es
+
+    # warm-ups (kernel loads, graph instantiation, workspaces)
     for K, P0, ne in zip(Ks[:4], P0s[:4], nes[:4]):
         solve(K, P0, ne, config=c64)
+        solve_scf(K, P0, ne, config=ref_scf)
     solve_batch(Ks, P0s, nes, config=c64, lanes=16)
-    solve_batch(Ks, P0s, nes, config=cmx, lanes=16)
-    t_one, E_one, r_one = [], [], []
-    torch.cuda.synchronize()
-    for K, P0, ne in zip(Ks, P0s, nes):
-        r, ms = ev_time(lambda: solve(K, P0, ne, config=c64))
-        t_one.append(ms)
-        E_one.append(float(r.energy))
-    E_one = np.array(E_one)
-    scan = {"n_solves": len(probs), "tol_E": 1e-9,
-            "fp64_solve_by_solve": {"solves_per_s": round(len(probs) / (sum(t_one) / 1e3), 2),
-                                    "total_ms": round(sum(t_one), 2),
-                                    "p50_ms": round(float(np.percentile(t_one, 50)), 2),
-                                    "p99_ms": round(float(np.percentile(t_one, 99)), 2)}}
-    for name, cfg in (("fp64_batched", c64), ("mixed_batched", cmx)):
-        (rb, tb), ms = median_run(lambda: solve_batch(Ks, P0s, nes, config=cfg, lanes=16, return_times=True), 3)
-        Eb = np.array([float(r.energy) for r in rb])
-        rel = np.abs(Eb - E_one) / np.abs(E_one)
-        scan[name] = {"solves_per_s": round(len(probs) / (ms / 1e3), 2), "total_ms": round(ms, 2),
-                      "p50_ms": round(float(np.percentile(tb, 50)), 2),
-                      "p99_ms": round(float(np.percentile(tb, 99)), 2), "lanes": 16,
-                      "max_rel_dE_vs_fp64": float(rel.max()), "n_rel_dE_above_1e-9": int((rel > 1e-9).sum()),
+    solve_scf_batch(Ks, P0s, nes, config=mixed_scf, workers=16)
+    solve_batch(Ks[:16], P0s[:16], nes[:16], config=mixed_cg, lanes=16)
+    scan = {"n_solves": len(probs), "oracle": "tests/golden/scan64_oracle.json (fixed point: oracle SCF-DIIS to 1e-11)"}
+    t_cg, E_cg = one_by_one(lambda K, P0, ne: solve(K, P0, ne, config=c64))
+    scan["fp64_solve_by_solve"] = {
+        "solver": "CG, tol_E 1e-9 (reference algorithm)", "solves_per_s": round(64 / (sum(t_cg) / 1e3), 2),
+        "total_ms": round(sum(t_cg), 2), "p50_ms": round(float(np.percentile(t_cg, 50)), 2),
+        "p99_ms": round(float(np.percentile(t_cg, 99)), 2),
+        "max_abs_dE_vs_oracle_reference_cg": float(np.abs(np.asarray(E_cg) - Ecg).max()), **errors(E_cg)}
+    t_scf, E_scf = one_by_one(lambda K, P0, ne: solve_scf(K, P0, ne, config=ref_scf))
+    scan["fp64_scf_solve_by_solve"] = {
+        "solver": "SCF-DIIS with the reference's steps (bisection mu, Jacobi eigh), density_tol 1e-8",
+        "solves_per_s": round(64 / (sum(t_scf) / 1e3), 2), "total_ms": round(sum(t_scf), 2),
+        "p50_ms": round(float(np.percentile(t_scf, 50)), 2), "p99_ms": round(float(np.percentile(t_scf, 99)), 2),
+        **errors(E_scf)}
+    legs = (("fp64_batched", "CG, tol_E 1e-9, 16 streams",
+             lambda: solve_batch(Ks, P0s, nes, config=c64, lanes=16, return_times=True)),
+            ("mixed_batched", "SCF-DIIS, FP32 exchange until density residual 1e-5 then FP64, Newton mu, warm eigh, "
+             "16 streams", lambda: solve_scf_batch(Ks, P0s, nes, config=mixed_scf, workers=16, return_times=True)),
+            ("mixed_cg_polish_batched", "FP32-exchange CG to tol_E 1e-6, then FP64 SCF-DIIS polish, 16 streams",
+             lambda: solve_batch(Ks, P0s, nes, config=mixed_cg, lanes=16, return_times=True)))
+    for name, desc, fn in legs:
+        (rb, tb), ms = median_run(fn, 3)
+        scan[name] = {"solver": desc, "solves_per_s": round(64 / (ms / 1e3), 2), "total_ms": round(ms, 2),
+                      "p50_ms": round(float(np.percentile(tb, 50)), 2), "p99_ms": round(float(np.percentile(tb, 99)), 2),
                       "all_converged": bool(all(bool(r.converged) for r in rb)),
-                      "speedup_vs_fp64_solve_by_solve": round(sum(t_one) / ms, 3)}
+                      "speedup_vs_fp64_solve_by_solve": round(sum(t_cg) / ms, 3),
+                      "speedup_vs_fp64_scf_solve_by_solve": round(sum(t_scf) / ms, 3),
+                      **errors([float(r.energy) for r in rb])}
     out["density_scan_64"] = scan
-    out["gradients_96x96_nb4"] = run_gradients(dev, ev_time)
+    out["gradients_96x96_nb4"] = run_gradients(dev, ev_time, base["newton_96x96_nb4"])
     import torch.distributed as dist
     if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
         # the 64 solves sharded over the ranks (greedy longest-first), FP64, batched per rank
@@ -408,14 +452,15 @@ def run_solves(dev):
         scan["fp64_sharded_over_ranks"] = {
             "ranks": dist.get_world_size(), "solves_per_s": round(len(probs) / (float(t) / 1e3), 2),
             "total_ms_max_over_ranks": round(float(t), 2),
-            "max_rel_dE_vs_fp64": float((np.abs(Es - E_one) / np.abs(E_one)).max())}
+            "max_abs_dE_vs_oracle_reference_cg": float(np.abs(Es - Ecg).max())}
     return out
 
 
-def run_gradients(dev, ev_time):
+def run_gradients(dev, ev_time, oracle=None):
     """96x96 nb=4 scalar-V model: trust-region Newton (tol_grad 1e-6) and SCF-DIIS solves, then
     d Omega*/d(U, d, h_R) through the hand-written adjoint at the converged density, with a
-    central difference of Omega in U at that density (step 1e-6) beside it."""
+    central difference of Omega in U at that density (step 1e-6) beside it.  ``oracle``: the
+    oracle's record for this problem (its own Newton result and the fixed point)."""
     import torch
     import jax_hf_b200 as G
     from jax_hf_b200 import adjoint as A
@@ -431,10 +476,17 @@ def run_gradients(dev, ev_time):
     rn, ms_n = ev_time(lambda: solve(K, P0, p3.n_electrons, config=ncfg))
     out["newton"] = {"ms_per_solve": round(ms_n, 2), "n_iter": int(rn.n_iter), "converged": bool(rn.converged),
                      "energy": float(rn.energy)}
+    if oracle is not None:
+        ra = oracle["reference_algorithm"]
+        out["newton"].update(oracle_n_iter=ra["n_iter"], oracle_converged=ra["converged"],
+                             rel_dE_vs_oracle_newton=abs(float(rn.energy) - ra["energy"]) / abs(ra["energy"]))
     scfg = SCFConfig(acceleration="diis", density_tol=1e-10, comm_tol=1e-9, max_iter=300)
     rs, ms_s = ev_time(lambda: solve_scf(K, P0, p3.n_electrons, config=scfg))
     out["scf_diis"] = {"ms_per_solve": round(ms_s, 2), "iterations": int(rs.iterations),
                        "converged": bool(rs.converged), "energy": float(rs.energy)}
+    if oracle is not None:
+        Ef = oracle["fixed_point_energy"]
+        out["scf_diis"]["rel_dE_vs_oracle_fixed_point"] = abs(float(rs.energy) - Ef) / abs(Ef)
     dens = rs.density_matrix if bool(rs.converged) else rn.density
     dV = S.coulomb_scalar_derivatives(96, 1.0, 2.0)
     R = S.lattice_vectors(2.0)
@@ -478,6 +530,9 @@ def _finish(args, ws, rank, value, dev_ms, avg_us, n_builds, t_wall, clocks, var
         "variants": variants,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one build's passes, "
+                                       "from the committed capture profiles/fock_build_192x192_nb8_c128_fast_passes.md "
+                                       "(not measured in this run)",
                      "algorithmic_bytes_per_build": ab, "peak_source": peak_kind},
         "e2e": None if e2e_val is None else {
             "value": round(e2e_val, 1), "unit": UNIT, "h2d_bytes_per_step": nbytes_state,
@@ -520,6 +575,15 @@ def cpu_baseline(P, prob, n=3):
                       f"on the same 192x192 nb=8 input; {dt:.3f} s per build"}
 
 
+def jax_probe() -> str:
+    """What importing the reference's dependency (JAX) gives on this machine."""
+    try:
+        import jax  # noqa: F401
+        return f"jax {jax.__version__} importable"
+    except Exception as exc:  # the reference cannot run without it
+        return f"import jax failed: {type(exc).__name__}: {exc}"
+
+
 def run_reference(args, ws, rank):
     if rank != 0:
         return None
@@ -533,8 +597,8 @@ def run_reference(args, ws, rank):
         fn()
     dt = time.perf_counter() - t
     val = args.steps / dt
-    sample = (f"each step = 1 oracle build_fock (NumPy/SciPy restatement of jax_hf's path; JAX is not "
-              f"installed) on the 192x192 nb=8 complex128 input, scipy.fft workers={cores}")
+    sample = (f"each step = 1 oracle build_fock (NumPy/SciPy restatement of jax_hf's path; jax_hf itself cannot "
+              f"run here: {jax_probe()}) on the 192x192 nb=8 complex128 input, scipy.fft workers={cores}")
     return {
         "impl": "reference", "metric": METRIC, "value": round(val, 4), "unit": UNIT, "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * dt / args.steps, 2),
