@@ -408,7 +408,7 @@ def run_solves(dev):
         solve(K, P0, ne, config=c64)
         solve_scf(K, P0, ne, config=ref_scf)
     solve_batch(Ks, P0s, nes, config=c64, lanes=16)
-    solve_scf_batch(Ks, P0s, nes, config=mixed_scf, workers=16)
+    solve_scf_batch(Ks, P0s, nes, config=mixed_scf, workers=8)
     solve_batch(Ks[:16], P0s[:16], nes[:16], config=mixed_cg, lanes=16)
     scan = {"n_solves": len(probs), "oracle": "tests/golden/scan64_oracle.json (fixed point: oracle SCF-DIIS to 1e-11)"}
     t_cg, E_cg = one_by_one(lambda K, P0, ne: solve(K, P0, ne, config=c64))
@@ -426,7 +426,7 @@ def run_solves(dev):
     legs = (("fp64_batched", "CG, tol_E 1e-9, 16 streams",
              lambda: solve_batch(Ks, P0s, nes, config=c64, lanes=16, return_times=True)),
             ("mixed_batched", "SCF-DIIS, FP32 exchange until density residual 1e-5 then FP64, Newton mu, warm eigh, "
-             "16 streams", lambda: solve_scf_batch(Ks, P0s, nes, config=mixed_scf, workers=16, return_times=True)),
+             "8 streams", lambda: solve_scf_batch(Ks, P0s, nes, config=mixed_scf, workers=8, return_times=True)),
             ("mixed_cg_polish_batched", "FP32-exchange CG to tol_E 1e-6, then FP64 SCF-DIIS polish, 16 streams",
              lambda: solve_batch(Ks, P0s, nes, config=mixed_cg, lanes=16, return_times=True)))
     for name, desc, fn in legs:

@@ -107,6 +107,7 @@ struct Scf {
   bool fp32 = false;    // this build runs the exchange FFT in FP32
   bool mu_warm = false;  // mu from the Newton-bracket solver started at the previous mu
   bool eig_warm = false; // eigh started from the eigenvectors in kV (the previous decomposition)
+  bool eig_cols = false; // eigh by the lane-per-column Jacobi (warm_eigh mode, nb <= 8)
   int fock(const void* P, void* Sg, void* H, void* F) {
     const unsigned flags = pb->fock_flags | (fp32 ? HF_FOCK_FFT_FP32 : 0u);
     return hf_fock_build(s, HF_C128, flags, pb->nk1, pb->nk2, nb, P, pb->h, pb->VR, pb->refP, pb->HH,
@@ -121,8 +122,9 @@ struct Scf {
   int density_from_fock(const void* F, void* P_out) {
     int st;
     double* sc = scal();
-    if (eig_warm) {
-      if ((st = hf_eigh_warm(s, nk, nb, F, at<void>(kV), at<void>(kV), at<double>(kEV)))) return st;
+    if (eig_cols) {  // lane-per-column Jacobi, from the previous eigenvectors when there are any
+      if ((st = hf_eigh_warm(s, nk, nb, F, eig_warm ? at<void>(kV) : nullptr, at<void>(kV), at<double>(kEV))))
+        return st;
     } else if ((st = hf_eigh(s, HF_C128, nk, nb, F, at<double>(kEV), at<void>(kV)))) {
       return st;
     }
@@ -256,7 +258,8 @@ extern "C" int hf_scf_solve(void* stream, const hf_cg_problem* pb, const hf_scf_
       }
     }
     S.mu_warm = cf->mu_method == 2 && k > 0;
-    S.eig_warm = cf->warm_eigh != 0 && nb <= 8 && k > 0;
+    S.eig_cols = cf->warm_eigh != 0 && nb <= 8;
+    S.eig_warm = S.eig_cols && k > 0;
     if ((st = S.build_and_occupy(density, F, Pn))) return st;
     const int kd = k - base;  // index in the current DIIS history
     void* R_out = diis ? (void*)(S.at<unsigned char>(kRH) + (size_t)(kd % nh) * qbytes) : (void*)S.at<void>(kRH);
@@ -363,7 +366,8 @@ extern "C" int hf_scf_solve(void* stream, const hf_cg_problem* pb, const hf_scf_
   // final build at the returned density (reference_scf.py:345-347), FP64 in every mode
   S.fp32 = false;
   S.mu_warm = cf->mu_method == 2 && k > 0;
-  S.eig_warm = cf->warm_eigh != 0 && nb <= 8 && k > 0;
+  S.eig_cols = cf->warm_eigh != 0 && nb <= 8;
+  S.eig_warm = S.eig_cols && k > 0;
   if ((st = S.build_and_occupy(density, fock, S.at<void>(kPN)))) return st;
   double fin[3] = {0.0, 0.0, 0.0};
   if ((st = S.read(fin, sc, 3))) return st;

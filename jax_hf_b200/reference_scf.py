@@ -345,6 +345,18 @@ def _solve_scf_native(kernel, P0, n_electrons, cfg):
                               "fp32_switch_iter": int(out[4]) if cfg.fp32_exchange else -1})
 
 
+_STREAMS: dict = {}
+
+
+def _worker_streams(dev, n):
+    """The first n streams of a per-device pool that lives as long as the process: the
+    solvers' workspaces are cached per stream, so reusing the streams reuses them."""
+    pool = _STREAMS.setdefault(str(dev), [])
+    while len(pool) < n:
+        pool.append(torch.cuda.Stream(dev))
+    return pool[:n]
+
+
 def solve_scf_batch(kernels, P0s, n_electrons, *, config: SCFConfig | None = None, workers: int = 16,
                     return_times: bool = False):
     """Many independent SCF solves at once (extension; density scans).
@@ -373,7 +385,7 @@ def solve_scf_batch(kernels, P0s, n_electrons, *, config: SCFConfig | None = Non
     main = torch.cuda.current_stream(dev)
     ready = torch.cuda.Event()
     ready.record(main)
-    streams = [torch.cuda.Stream(dev) for _ in range(max(1, min(int(workers), n)))]
+    streams = _worker_streams(dev, max(1, min(int(workers), n)))
 
     def work(stream):
         try:
