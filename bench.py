@@ -139,10 +139,17 @@ def run_ours(args, ws, rank, local):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream()
 
-    def timed_builds(n, fn):
+    flush_words = flush.view(torch.float32)
+
+    def timed_builds(n, fn, read_flush=False):
+        # L2 flush before every build: a 256 MiB write (the headline), or a 256 MiB read, which
+        # leaves no dirty lines whose write-back would land inside the timed build
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
         for i in range(n):
-            flush.fill_(i & 0xFF)
+            if read_flush:
+                flush_words.sum()
+            else:
+                flush.fill_(i & 0xFF)
             ev[i][0].record(stream)
             fn()
             ev[i][1].record(stream)
@@ -190,12 +197,16 @@ def run_ours(args, ws, rank, local):
                 contact_g=a64["contact_g"], contact_Oi=a64["contact_Oi"], contact_Oj=a64["contact_Oj"])
     S64, F64 = torch.empty_like(P64), torch.empty_like(P64)
     H64 = torch.empty((1, 1, NB, NB), dtype=P64.dtype, device=dev)
-    for name, fn, nbytes in (
-        ("c64", lambda: G.build_fock(P64, out=(S64, H64, F64), **kw64), alg_bytes(NK, NK, NB, 8)),
-        ("c128_fp32fft", lambda: G.build_fock(P, out=(Sg, H, F), fft_precision="fp32", **kw), alg_bytes(NK, NK, NB)),
+    for name, fn, nbytes, rf in (
+        ("c64", lambda: G.build_fock(P64, out=(S64, H64, F64), **kw64), alg_bytes(NK, NK, NB, 8), False),
+        ("c128_fp32fft", lambda: G.build_fock(P, out=(Sg, H, F), fft_precision="fp32", **kw), alg_bytes(NK, NK, NB),
+         False),
+        ("c128_read_flush", build, alg_bytes(NK, NK, NB), True),
+        ("c128_pipe_engine", lambda: G.build_fock(P, out=(Sg, H, F), engine="pipe", **kw), alg_bytes(NK, NK, NB),
+         False),
     ):
-        timed_builds(8, fn)
-        ev = timed_builds(STEP_BUILDS, fn)
+        timed_builds(8, fn, rf)
+        ev = timed_builds(STEP_BUILDS, fn, rf)
         torch.cuda.synchronize()
         t = [s.elapsed_time(e) for (s, e) in ev]
         us = 1e3 * float(np.mean(t))

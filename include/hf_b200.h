@@ -267,6 +267,9 @@ int hf_qr_retract(void* stream, int dtype, int batch, int nb, const void* G, dou
  *  hf_scf_residuals  comm = F P - P F, delta = Pn - P and sums3 = {sum w|delta|^2, sum w|comm|^2,
  *                    sum w Re tr(F delta)}  (reference_scf.py:291-295, 319-320)
  *  hf_gram           DIIS B_ij = sum_k w Re tr(R_i^H R_j), upper triangle row-major (reference_scf.py:110-111)
+ *  hf_gram_row       b_j = B_ij for one i and every j < n (n <= 16): the row of B that changes when DIIS
+ *                    replaces history slot i; each entry equals hf_gram's bit for bit (extension, no
+ *                    reference counterpart; the reference recomputes all of B each step)
  *  hf_lincomb        out = sum_i c_i X_i, c on device (reference_scf.py:305)
  *  hf_axpby          out = [herm](a x + b y); hf_axpby_real the same for real vectors
  *  hf_jdot           sum_k wX sum Re(conj(aX) bX) + sum_k wp sum ap bp (solver.py:205-233, 783-787)
@@ -284,6 +287,8 @@ int hf_scf_residuals(void* stream, int nk, int nb, const void* F, const void* P,
                      void* comm, void* delta, double* sums3, void* ws);
 int hf_gram(void* stream, int n, size_t stride, int nk, int nb, const void* R, const double* w, double* B_out,
             void* ws);
+int hf_gram_row(void* stream, int n, int i, size_t stride, int nk, int nb, const void* R, const double* w,
+                double* b_out, void* ws);
 int hf_lincomb(void* stream, int n, size_t stride, size_t len, const void* X, const double* c, void* out);
 int hf_axpby(void* stream, size_t nk, int nb, double a, const void* x, double b, const void* y, int herm,
              void* out);
@@ -405,6 +410,37 @@ int hf_scf_workspace_size(const hf_cg_problem* problem, const hf_scf_config* con
 int hf_scf_solve(void* stream, const hf_cg_problem* problem, const hf_scf_config* config, const void* P0,
                  void* density, void* fock, double* hist_E, double* hist_D, double* hist_C, double* scalars_out,
                  void* workspace, size_t workspace_bytes);
+
+/* ---- Trust-region Newton driver (complex128) -----------------------------------
+ * Replaces jax_hf.solve with optimizer="newton" (solver.py:686-1078) for
+ * project_fn=None, block_sizes=None and the built-in Fock build (nb <= 16):
+ * Steihaug truncated CG on the joint (Q, p) Hessian, Cayley trial steps,
+ * trust-region updates and the Gaussian deflation bias (solver.py:799-812).
+ * SolverConfig fields as solver.py:240-286; tol_grad <= 0 means 1e-6
+ * (solver.py:1191).  deflation_targets: n_deflation (nk1, nk2, nb, nb)
+ * complex128 device arrays back to back (used when n_deflation > 0 and
+ * deflation_sigma > 0).  The problem is an hf_cg_problem (sigma_buf / h_buf
+ * unused).  Outputs: Q (nk1, nk2, nb, nb) complex128, p (nk1, nk2, nb) float64,
+ * density and fock (device, as SolveResult), hist_E / hist_G (HOST float64,
+ * max_iter entries, may be NULL) and scalars_out (HOST, 6 float64): mu,
+ * energy, n_iter, converged, last grad_norm, Fock builds.  The host reads the
+ * loop's reductions in small batches: two reads per inner CG step, three or
+ * four per outer step. */
+typedef struct hf_newton_config {
+  int max_iter;
+  double tol_grad, denom_scale;
+  int mu_maxiter;
+  double tr_delta0;
+  int tr_cg_max;
+  int n_deflation;
+  const void* deflation_targets;
+  double deflation_sigma, deflation_length;
+} hf_newton_config;
+
+int hf_newton_workspace_size(const hf_cg_problem* problem, const hf_newton_config* config, size_t* bytes);
+int hf_newton_solve(void* stream, const hf_cg_problem* problem, const hf_newton_config* config, const void* P0,
+                    void* Q, void* p, void* density, void* fock, double* hist_E, double* hist_G,
+                    double* scalars_out, void* workspace, size_t workspace_bytes);
 
 /* ---- Reverse mode (complex128) -------------------------------------------------
  * The reference differentiates build_fock / hf_energy / free_energy with

@@ -74,6 +74,7 @@ _SIGS = {
     "hf_fermi": ([vp, sz, vp, vp, f64, i32, f64, vp], i32),
     "hf_scf_residuals": ([vp, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp], i32),
     "hf_gram": ([vp, i32, sz, i32, i32, vp, vp, vp, vp], i32),
+    "hf_gram_row": ([vp, i32, i32, sz, i32, i32, vp, vp, vp, vp], i32),
     "hf_lincomb": ([vp, i32, sz, sz, vp, vp, vp], i32),
     "hf_axpby": ([vp, sz, i32, f64, vp, f64, vp, i32, vp], i32),
     "hf_axpby_real": ([vp, sz, f64, vp, f64, vp, vp], i32),
@@ -90,6 +91,8 @@ _SIGS = {
     "hf_cg_batch_workspace_size": ([vp, i32, vp, psz], i32),
     "hf_scf_workspace_size": ([vp, vp, psz], i32),
     "hf_scf_solve": ([vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, sz], i32),
+    "hf_newton_workspace_size": ([vp, vp, psz], i32),
+    "hf_newton_solve": ([vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, sz], i32),
     "hf_fock_vjp_workspace_size": ([i32, u32, i32, i32, i32, psz], i32),
     "hf_fock_build_vjp": ([vp, i32, u32, i32, i32, i32, vp, vp, vp, vp, vp, vp, sz], i32),
     "hf_energy_vjp": ([vp, i32, i32, i32, vp, vp, vp, vp, i32, vp, f64, vp, vp, vp], i32),

@@ -15,6 +15,8 @@ void set_error(const std::string& msg);
 int fail(int status, const std::string& msg);
 int cuda_check(cudaError_t e, const char* what);
 int allow_max_dynamic_smem(const void* fn);
+int context_id(unsigned long long* id);
+int symbol_address(const void* symbol, void** out);
 
 #define HF_SMEM_CAP(...)                                              \
   do {                                                                \

@@ -488,25 +488,15 @@ static int launch_fock(FockParams& p, cudaStream_t stream, bool need_consts) {
 }
 
 // ------------------------------------------------------------ fault word -----
-// Written by the bounded waits of the pipelined passes (fock_pipe.cuh).  Its
-// address is looked up once per device; the lookup does not survive a reset of
-// the device's primary context (cudaDeviceReset) within the process.
+// Written by the bounded waits of the pipelined passes (fock_pipe.cuh).  Its address
+// is cached per context (hf::symbol_address), so a device reset gets a fresh lookup.
 __device__ int g_fock_fault;
-static std::mutex g_fault_mu;
-static std::map<int, int*> g_fault_ptr;
 
 static int fault_word(int** out) {
-  int dev = 0;
-  HF_CUDA(cudaGetDevice(&dev));
-  std::lock_guard<std::mutex> lk(g_fault_mu);
-  auto it = g_fault_ptr.find(dev);
-  if (it == g_fault_ptr.end()) {
-    void* ptr = nullptr;
-    HF_CUDA(cudaGetSymbolAddress(&ptr, g_fock_fault));
-    it = g_fault_ptr.emplace(dev, static_cast<int*>(ptr)).first;
-  }
-  *out = it->second;
-  return HF_OK;
+  void* p = nullptr;
+  int st = hf::symbol_address(reinterpret_cast<const void*>(&g_fock_fault), &p);
+  *out = static_cast<int*>(p);
+  return st;
 }
 
 // ------------------------------------------------------------ autotuner -----

@@ -441,16 +441,16 @@ int hf::find_mu_internal(void* stream, int dtype, int method, int nk1, int nk2, 
   const void* fn = threads == 256 ? (single ? (const void*)k_find_mu<float, 256> : (const void*)k_find_mu<double, 256>)
                                   : (single ? (const void*)k_find_mu<float, kMuThreads>
                                             : (const void*)k_find_mu<double, kMuThreads>);
-  int dev = 0;
-  HF_CUDA(cudaGetDevice(&dev));
-  // per (kernel, device), set up once under a lock: the largest schedulable cluster
+  unsigned long long ctx = 0;
+  if (int cst = context_id(&ctx)) return cst;
+  // per (kernel, context), set up once under a lock: the largest schedulable cluster
   // size (beyond the portable 8 only as large as the device can co-schedule) and the
   // opt-in for the shared-memory cache of the largest block
   static std::mutex mu_setup;
-  static std::map<std::pair<const void*, int>, int> max_cluster;
+  static std::map<std::pair<const void*, unsigned long long>, int> max_cluster;
   {
     std::lock_guard<std::mutex> lk(mu_setup);
-    auto key = std::make_pair(fn, dev);
+    auto key = std::make_pair(fn, ctx);
     auto it = max_cluster.find(key);
     if (it == max_cluster.end()) {
       int mc = 8;

@@ -146,6 +146,38 @@ __global__ void k_gram(size_t stride, size_t len, int nb2, const double2* __rest
   }
 }
 
+// One row of the DIIS Gram matrix: b[j] = sum_k w_k Re tr(R_i^H R_j) for j < N and a
+// fixed i.  A DIIS step replaces one history slot, so only that slot's row changes;
+// the SCF driver keeps the rest of B and refreshes the row with one launch.  Every
+// entry is formed exactly as in k_gram (fma(x_i, x_j, y_i y_j) is symmetric in i, j).
+template <int N>
+__global__ void k_gram_row(size_t stride, size_t len, int nb2, const double2* __restrict__ R, int inew,
+                           const double* __restrict__ w, double* part) {
+  __shared__ double red[64];
+  double acc[N];
+#pragma unroll
+  for (int q = 0; q < N; ++q) acc[q] = 0.0;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < len; e += (size_t)gridDim.x * blockDim.x) {
+    const double wk = w[e / nb2];
+    const double2 a = R[inew * stride + e];
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+      const double2 b = R[j * stride + e];
+      acc[j] = fma(wk, fma(a.x, b.x, a.y * b.y), acc[j]);
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < N; ++q) {
+    KSum t;
+    t.add(acc[q]);
+    KSum rr = block_reduce(t, red);
+    if (threadIdx.x == 0) {
+      part[((size_t)blockIdx.x * N + q) * 2] = rr.s;
+      part[((size_t)blockIdx.x * N + q) * 2 + 1] = rr.c;
+    }
+  }
+}
+
 // out = sum_i c_i X_i (+ optional herm)
 __global__ void k_lincomb(int n, size_t stride, size_t len, int nb, const double2* __restrict__ X,
                           const double* __restrict__ c, double2* __restrict__ out) {
@@ -448,6 +480,25 @@ extern "C" int hf_gram(void* stream, int n, size_t stride, int nk, int nb, const
 #undef HF_GRAM
   }
   return finish(HF_S, (double*)ws, g, n * (n + 1) / 2, B_out);
+}
+
+extern "C" int hf_gram_row(void* stream, int n, int i, size_t stride, int nk, int nb, const void* R,
+                           const double* w, double* b_out, void* ws) {
+  if (n < 1 || n > 16 || i < 0 || i >= n || !R || !w || !b_out || !ws)
+    return fail(HF_ERR_INVALID, "hf_gram_row: 1 <= n <= 16, 0 <= i < n");
+  const size_t len = (size_t)nk * nb * nb;
+  const int g = nblocks(len);
+  switch (n) {
+#define HF_GRAM_ROW(N)                                                                                    \
+  case N:                                                                                                 \
+    k_gram_row<N><<<g, kOpsThreads, 0, HF_S>>>(stride, len, nb * nb, (const double2*)R, i, w, (double*)ws); \
+    break;
+    HF_GRAM_ROW(1) HF_GRAM_ROW(2) HF_GRAM_ROW(3) HF_GRAM_ROW(4) HF_GRAM_ROW(5) HF_GRAM_ROW(6) HF_GRAM_ROW(7)
+    HF_GRAM_ROW(8) HF_GRAM_ROW(9) HF_GRAM_ROW(10) HF_GRAM_ROW(11) HF_GRAM_ROW(12) HF_GRAM_ROW(13)
+    HF_GRAM_ROW(14) HF_GRAM_ROW(15) HF_GRAM_ROW(16)
+#undef HF_GRAM_ROW
+  }
+  return finish(HF_S, (double*)ws, g, n, b_out);
 }
 
 extern "C" int hf_lincomb(void* stream, int n, size_t stride, size_t len, const void* X, const double* c, void* out) {

@@ -31,6 +31,7 @@ enum {
 
 // device scalar block (float64): mu_raw, mu, E, E_new, sums[3], red[1], gram[21], coeff[n]
 constexpr int kSMuRaw = 0, kSMu = 1, kSE = 2, kSEnew = 3, kSSums = 4, kSRed = 7, kSGram = 8, kSCoeff = 29;
+static_assert(kSGram + 21 <= kSCoeff, "the Gram slots hold 21 entries (n = 6 upper triangle, or a row of n <= 16)");
 
 size_t scf_layout(const hf_cg_problem& pb, const hf_scf_config& cf, size_t fock_ws, size_t red_ws, size_t ops_ws,
                   ScfLayout& L) {
@@ -241,6 +242,8 @@ extern "C" int hf_scf_solve(void* stream, const hf_cg_problem* pb, const hf_scf_
     HF_CUDA(cudaMemsetAsync(S.at<void>(kFHIST), 0, (size_t)nh * qbytes, s));
   }
   std::vector<double> hv(kSCoeff + 8, 0.0);
+  // nh > 6: B is kept here between iterations and one row (the replaced slot's) is refreshed per step
+  std::vector<double> Bkeep(diis && nh > 6 ? (size_t)nh * nh : 0, 0.0);
   int k = 0, base = 0, switch_iter = -1;  // base: first iteration of the current DIIS history
   bool converged = false;
   double d_prev = INFINITY;
@@ -255,6 +258,7 @@ extern "C" int hf_scf_solve(void* stream, const hf_cg_problem* pb, const hf_scf_
       if (diis) {
         HF_CUDA(cudaMemsetAsync(S.at<void>(kRH), 0, (size_t)nh * qbytes, s));
         HF_CUDA(cudaMemsetAsync(S.at<void>(kFHIST), 0, (size_t)nh * qbytes, s));
+        std::fill(Bkeep.begin(), Bkeep.end(), 0.0);
       }
     }
     S.mu_warm = cf->mu_method == 2 && k > 0;
@@ -270,6 +274,8 @@ extern "C" int hf_scf_solve(void* stream, const hf_cg_problem* pb, const hf_scf_
                               cudaMemcpyDeviceToDevice, s));
       if (nh <= 6) {
         if ((st = hf_gram(s, nh, nq, nk, nb, S.at<void>(kRH), w2d, sc + kSGram, ops))) return st;
+      } else if ((st = hf_gram_row(s, nh, kd % nh, nq, nk, nb, S.at<void>(kRH), w2d, sc + kSGram, ops))) {
+        return st;
       }
     }
     if ((st = S.read(hv.data(), sc, kSCoeff))) return st;
@@ -286,16 +292,9 @@ extern "C" int hf_scf_solve(void* stream, const hf_cg_problem* pb, const hf_scf_
         for (int i = 0; i < nh; ++i)
           for (int j = i; j < nh; ++j, ++q) B[i * nh + j] = B[j * nh + i] = hv[kSGram + q];
       } else {
-        for (int i = 0; i < nh; ++i)
-          for (int j = i; j < nh; ++j) {
-            if ((st = hf_jdot(s, (size_t)nk, nb, S.at<unsigned char>(kRH) + (size_t)i * qbytes,
-                              S.at<unsigned char>(kRH) + (size_t)j * qbytes, w2d, nullptr, nullptr, nullptr,
-                              sc + kSRed, ops)))
-              return st;
-            double v = 0.0;
-            if ((st = S.read(&v, sc + kSRed, 1))) return st;
-            B[i * nh + j] = B[j * nh + i] = v;
-          }
+        const int i = kd % nh;
+        for (int j = 0; j < nh; ++j) Bkeep[(size_t)i * nh + j] = Bkeep[(size_t)j * nh + i] = hv[kSGram + j];
+        B = Bkeep;
       }
       double bmax = 0.0;
       for (double v : B) bmax = std::fmax(bmax, std::fabs(v));

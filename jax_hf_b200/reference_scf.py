@@ -189,7 +189,7 @@ def solve_scf(kernel, P0, n_electrons: float, *, config: SCFConfig | None = None
     comm_buf = torch.empty((nk1, nk2, nb, nb), dtype=cd, device=dev)
     delta = torch.empty_like(comm_buf)
     sums = torch.empty(3, dtype=torch.float64, device=dev)
-    gram = torch.empty(64, dtype=torch.float64, device=dev)
+    gram = torch.empty(256, dtype=torch.float64, device=dev)
     coeff_dev = torch.empty(max(n_hist, 1), dtype=torch.float64, device=dev)
     hE, hD, hC = [], [], []
     density = torch.as_tensor(P0).to(dev, cd).contiguous() if not (
@@ -440,9 +440,16 @@ def _gram_matrix(ops, R_hist, n, stride, w2d, gram):
                 B[i, j] = B[j, i] = g[q]
                 q += 1
         return B
+    if n > 16:
+        for i in range(n):
+            for j in range(i, n):
+                _lib.check(ops.L.hf_jdot(ops.s, ops.nk, ops.nb, R_hist[i].data_ptr(), R_hist[j].data_ptr(),
+                                         w2d.data_ptr(), None, None, None, gram.data_ptr(), ops.ws.data_ptr()))
+                B[i, j] = B[j, i] = float(gram[0])
+        return B
+    # n = 7 .. 16: one row per launch, all rows read back at once
     for i in range(n):
-        for j in range(i, n):
-            _lib.check(ops.L.hf_jdot(ops.s, ops.nk, ops.nb, R_hist[i].data_ptr(), R_hist[j].data_ptr(),
-                                     w2d.data_ptr(), None, None, None, gram.data_ptr(), ops.ws.data_ptr()))
-            B[i, j] = B[j, i] = float(gram[0])
-    return B
+        _lib.check(ops.L.hf_gram_row(ops.s, n, i, stride, ops.nk, ops.nb, R_hist.data_ptr(), w2d.data_ptr(),
+                                     gram[i * n:].data_ptr(), ops.ws.data_ptr()))
+    g = gram[: n * n].cpu().numpy().reshape(n, n)
+    return np.triu(g) + np.triu(g, 1).T

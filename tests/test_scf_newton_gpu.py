@@ -1,6 +1,8 @@
 """GPU parity of solve_scf (linear / DIIS / ODA), trust-region Newton, block specs and
 solver hooks against the CPU oracle (same FP64 algorithms, same starting points)."""
 
+import ctypes
+
 import numpy as np
 import pytest
 import torch
@@ -69,6 +71,10 @@ SCF_CASES = [
                                              trust_radius=0.5)),
     ("dirac_diis_damp_shift", "dirac", 16.0, dict(max_iter=800, density_tol=1e-6, comm_tol=1e-5,
                                                   acceleration="diis", diis_damping=0.7, level_shift=0.3)),
+    # history sizes 7-16 take the one-row Gram update; on this model the oracle's own iteration
+    # count moves by at most 1-2 under 1e-15 relative perturbations of the residuals
+    ("diis10_24x24_nb4", "scf24", 2.0, dict(acceleration="diis", diis_size=10)),
+    ("diis16_24x24_nb4", "scf24", 2.0, dict(acceleration="diis", diis_size=16)),
 ]
 
 
@@ -132,6 +138,39 @@ def test_native_scf_driver_matches_python_loop(cuda, monkeypatch, name, model, n
     assert a.message.split()[0] == b.message.split()[0]
 
 
+@pytest.mark.parametrize("n", [1, 4, 6, 7, 11, 16])
+def test_gram_row_matches_gram(cuda, n):
+    """hf_gram_row: row i of the DIIS Gram matrix.  For n <= 6 every entry equals hf_gram's bit
+    for bit; for every n it matches a float64 torch sum to 1e-13 relative."""
+    from jax_hf_b200 import _lib
+    L = _lib.lib()
+    g = torch.Generator(device="cpu").manual_seed(n)
+    nk, nb = 1500, 5
+    R = torch.randn(n, nk, nb, nb, dtype=torch.complex128, generator=g).cuda()
+    w = torch.rand(nk, dtype=torch.float64, generator=g).cuda()
+    ws_bytes = ctypes.c_size_t(0)
+    _lib.check(L.hf_ops_workspace_size(ctypes.byref(ws_bytes)))
+    ws = torch.empty(ws_bytes.value, dtype=torch.uint8, device="cuda")
+    s = _lib.stream_ptr(R.device)
+    stride = nk * nb * nb
+    rows = torch.empty(n, n, dtype=torch.float64, device="cuda")
+    for i in range(n):
+        _lib.check(L.hf_gram_row(s, n, i, stride, nk, nb, R.data_ptr(), w.data_ptr(), rows[i].data_ptr(),
+                                 ws.data_ptr()))
+    Rf = R.reshape(n, nk, -1)
+    ref = torch.einsum("k,ikm,jkm->ij", w, Rf.real, Rf.real) + torch.einsum("k,ikm,jkm->ij", w, Rf.imag, Rf.imag)
+    torch.cuda.synchronize()
+    assert float((rows - ref).abs().max()) <= 1e-13 * float(ref.abs().max())
+    assert torch.equal(rows, rows.T)
+    if n <= 6:
+        tri = torch.empty(n * (n + 1) // 2, dtype=torch.float64, device="cuda")
+        _lib.check(L.hf_gram(s, n, stride, nk, nb, R.data_ptr(), w.data_ptr(), tri.data_ptr(), ws.data_ptr()))
+        iu = torch.triu_indices(n, n)
+        assert torch.equal(rows[iu[0], iu[1]], tri)
+    assert L.hf_gram_row(s, 17, 0, stride, nk, nb, R.data_ptr(), w.data_ptr(), rows.data_ptr(),
+                         ws.data_ptr()) == _lib.HF_ERR_INVALID
+
+
 def test_scf_config_validation():
     from jax_hf_b200.reference_scf import SCFConfig
     with pytest.raises(ValueError, match="acceleration"):
@@ -159,6 +198,49 @@ def test_newton_matches_oracle(cuda, name, kw, ne, cfg):
     assert abs(float(r.energy) - Eo) <= 1e-9 * max(1.0, abs(Eo))
     assert np.abs(r.density.cpu().numpy() - ro["density"]).max() < 1e-6
     assert abs(int(r.n_iter) - ro["n_iter"]) <= 2
+
+
+@pytest.mark.parametrize("name,kw,ne,cfg", NEWTON_CASES, ids=[c[0] for c in NEWTON_CASES])
+def test_native_newton_driver_matches_python_loop(cuda, monkeypatch, name, kw, ne, cfg):
+    """hf_newton_solve issues the same device operations as the Python loop (newton.py) and
+    reads the same reductions, only in batches: the same steps, iteration for iteration."""
+    from jax_hf_b200 import newton
+    from jax_hf_b200.solver import SolverConfig, solve
+    K, _ = _kernels(kw)
+    P0 = torch.zeros(np.asarray(kw["hamiltonian"]).shape, dtype=torch.complex128, device="cuda")
+    res = {}
+    for native in (True, False):
+        monkeypatch.setattr(newton, "USE_NATIVE", native)
+        res[native] = solve(K, P0, ne, config=SolverConfig(**cfg))
+    a, b = res[True], res[False]
+    assert bool(a.converged) == bool(b.converged)
+    assert int(a.n_iter) == int(b.n_iter)
+    assert a.history["n_builds"] == b.history["n_builds"]
+    n = int(a.n_iter)
+    np.testing.assert_allclose(a.history["E"][:n].numpy(), b.history["E"][:n].numpy(), rtol=1e-13, atol=1e-13)
+    np.testing.assert_allclose(a.history["grad_norm"][:n].numpy(), b.history["grad_norm"][:n].numpy(),
+                               rtol=1e-9, atol=1e-14)
+    assert abs(float(a.energy) - float(b.energy)) <= 1e-12 * max(1.0, abs(float(b.energy)))
+    assert float((a.density - b.density).abs().max()) < 1e-10
+    assert abs(float(a.mu) - float(b.mu)) < 1e-10
+
+
+def test_native_newton_deflation_matches_python_loop(cuda, monkeypatch):
+    from jax_hf_b200 import newton
+    from jax_hf_b200.solver import SolverConfig, solve
+    K, _ = _kernels(_bistable())
+    P0 = torch.zeros((1, 1, 2, 2), dtype=torch.complex128, device="cuda")
+    r = solve(K, P0, 1.0, config=SolverConfig(optimizer="newton", tol_grad=1e-8, max_iter=100))
+    cfg = SolverConfig(optimizer="newton", tol_grad=1e-8, max_iter=200, deflation_targets=r.density,
+                       deflation_sigma=2.0, deflation_length=0.5)
+    res = {}
+    for native in (True, False):
+        monkeypatch.setattr(newton, "USE_NATIVE", native)
+        res[native] = solve(K, P0 + 0.0, 1.0, config=cfg)
+    a, b = res[True], res[False]
+    assert int(a.n_iter) == int(b.n_iter) and bool(a.converged) == bool(b.converged)
+    assert abs(float(a.energy) - float(b.energy)) <= 1e-12
+    assert float((a.density - b.density).abs().max()) < 1e-10
 
 
 def test_newton_bistable_and_deflation(cuda):

@@ -6,8 +6,10 @@ stream capture, where cudaMalloc is refused or synchronises the device.  For
 them the library offers a Fock build whose scratch is a fixed static device
 array.  This test calls it through the C ABI and checks that two calls in a
 row give the same Sigma, H and F as hf_fock_build with a caller workspace
-(relative tolerance 1e-12, as for every complex128 parity test), and that a
-mesh larger than the array is refused with an error instead of running.
+(relative tolerance 1e-12, as for every complex128 parity test), that the call
+captured in a CUDA graph after one eager call replays correctly on new inputs,
+and that a mesh larger than the array is refused with an error instead of
+running.
 
 The file is named so that pytest collects it last; it also passes when run on
 its own in a fresh process.
@@ -78,6 +80,62 @@ def test_static_scratch_matches_workspace_build_twice(cuda):
         for r, o in zip(ref, out):
             assert torch.isfinite(o).all()
             assert _rel(o, r) <= 1e-12
+
+
+def test_static_scratch_under_stream_capture(cuda):
+    """The use the entry point exists for: one eager call (loads the module, caches the scratch
+    address), then the call captured in a CUDA graph.  Replays on new inputs written into the
+    captured buffers agree with hf_fock_build at 1e-12."""
+    import jax_hf_b200 as G
+    from jax_hf_b200 import _lib
+
+    L = _lib.lib()
+    d = _inputs(31)
+    K = G.HartreeFockKernel(d["w"], d["h"], d["Vq"], 0.1, include_hartree=True, reference_density=d["refP"],
+                            hartree_matrix=d["HH"], contact_terms=[(0.25, d["Oa"], d["Oa"].conj().T)])
+    nk1, nk2, nb = K.shape
+    flags = _lib.FOCK_EXCHANGE | _lib.FOCK_HARTREE | _lib.FOCK_HAS_REFP
+    VR = K._VR_shifted
+    if not VR.is_complex():
+        flags |= _lib.FOCK_VR_REAL
+    P = torch.as_tensor(d["P"], device="cuda")
+    outs = [torch.empty_like(P), torch.empty((nb, nb), dtype=P.dtype, device="cuda"), torch.empty_like(P)]
+
+    def call(stream):
+        return L.hf_fock_build_static_scratch(stream, _lib.HF_C128, flags, nk1, nk2, nb, P.data_ptr(),
+                                              K.h.data_ptr(), VR.data_ptr(), K.refP.data_ptr(), K.HH.data_ptr(),
+                                              K.w2d.data_ptr(), 1, K.contact_g.data_ptr(),
+                                              K.contact_Oi.data_ptr(), K.contact_Oj.data_ptr(),
+                                              outs[0].data_ptr(), outs[1].data_ptr(), outs[2].data_ptr())
+
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        _lib.check(call(side.cuda_stream))  # the eager warm-up call, outside capture
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=side):
+        st = call(side.cuda_stream)
+    _lib.check(st)
+    need = C.c_size_t(0)
+    _lib.check(L.hf_fock_workspace_size(_lib.HF_C128, flags, nk1, nk2, nb, C.byref(need)))
+    ws = torch.empty(need.value, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    for seed in (41, 42):
+        P.copy_(torch.as_tensor(S.haar_density(48, nb, seed)[:nk1, :nk2], device="cuda"))
+        for o in outs:
+            o.fill_(float("nan"))
+        graph.replay()
+        ref = [torch.empty_like(o) for o in outs]
+        _lib.check(L.hf_fock_build(stream, _lib.HF_C128, flags, nk1, nk2, nb, P.data_ptr(), K.h.data_ptr(),
+                                   VR.data_ptr(), K.refP.data_ptr(), K.HH.data_ptr(), K.w2d.data_ptr(), 1,
+                                   K.contact_g.data_ptr(), K.contact_Oi.data_ptr(), K.contact_Oj.data_ptr(),
+                                   ref[0].data_ptr(), ref[1].data_ptr(), ref[2].data_ptr(), ws.data_ptr(),
+                                   ws.numel()))
+        torch.cuda.synchronize()
+        for r, o in zip(ref, outs):
+            assert torch.isfinite(o).all()
+            assert _rel(o, r) <= 1e-12
+    del graph
 
 
 def test_static_scratch_rejects_oversized_mesh(cuda):
