@@ -3,10 +3,17 @@
 Steihaug truncated CG on the joint (Q, p) Hessian; every Hessian-vector product
 is one Fock build of the linear response (refP = 0) plus two per-k kernels
 (`hf_newton_dP`, `hf_newton_hvp`).  Vectors, products and reductions run in the
-CUDA library in float64; the trust-region and CG scalars are read back once per
-reduction and the branch logic runs on the host, line for line with the
-reference loop body.  Deflation (the Gaussian bias of solver.py:799-812) is
+CUDA library in float64.  Deflation (the Gaussian bias of solver.py:799-812) is
 supported.
+
+Two drivers issue the same device operations in the same order:
+
+* the library's C++ driver ``hf_newton_solve`` (the default without hooks:
+  project_fn, block_sizes and fock_build_fn all None, nb <= 16), which reads
+  the loop's reductions in small batches (two reads per inner CG step);
+* the Python loop below (with hooks, or ``USE_NATIVE = False``), which reads
+  every reduction as it comes and runs the branch logic line for line with the
+  reference loop body.
 """
 
 from __future__ import annotations
@@ -70,10 +77,81 @@ class _V:
         _lib.check(self.L.hf_sub_scalar(self.s, x.numel(), x.data_ptr(), wsum_dev.data_ptr(), 1.0 / den))
 
 
+# solve_newton runs the library's Newton driver (hf_newton_solve) when no hook is given;
+# tests switch this off to compare it with the Python loop over the same device operations.
+USE_NATIVE = True
+
+
+class _NewtonConfig(C.Structure):
+    _fields_ = [("max_iter", C.c_int), ("tol_grad", C.c_double), ("denom_scale", C.c_double),
+                ("mu_maxiter", C.c_int), ("tr_delta0", C.c_double), ("tr_cg_max", C.c_int),
+                ("n_deflation", C.c_int), ("deflation_targets", C.c_void_p), ("deflation_sigma", C.c_double),
+                ("deflation_length", C.c_double)]
+
+
+def _deflation_targets(cfg, dev, shape):
+    targets = torch.as_tensor(cfg.deflation_targets).to(dev, torch.complex128)
+    if targets.ndim == 4:
+        targets = targets[None]
+    if targets.ndim != 5 or tuple(targets.shape[1:]) != tuple(shape):
+        raise ValueError("deflation_targets must have shape (n_solutions, nk1, nk2, nb, nb) matching the kernel; "
+                         f"got {tuple(targets.shape)}.")
+    return targets.contiguous()
+
+
+def _solve_newton_native(kernel, P0, n_electrons, cfg):
+    from .solver import KernelC128, SolveResult, _CgProblem
+    L = _lib.lib()
+    if not getattr(L, "_newton_bound", False):
+        L.hf_newton_workspace_size.argtypes = [C.POINTER(_CgProblem), C.POINTER(_NewtonConfig),
+                                               C.POINTER(C.c_size_t)]
+        L.hf_newton_workspace_size.restype = C.c_int
+        L.hf_newton_solve.argtypes = [C.c_void_p, C.POINTER(_CgProblem), C.POINTER(_NewtonConfig)] + \
+            [C.c_void_p] * 9 + [C.c_size_t]
+        L.hf_newton_solve.restype = C.c_int
+        L._newton_bound = True
+    dev = kernel.device
+    nk1, nk2, nb = kernel.shape
+    cd, rd = torch.complex128, torch.float64
+    kc = KernelC128(kernel)
+    pb = kc.problem(n_electrons)
+    has_defl = cfg.deflation_targets is not None and float(cfg.deflation_sigma) > 0.0
+    targets = _deflation_targets(cfg, dev, (nk1, nk2, nb, nb)) if has_defl else None
+    nc = _NewtonConfig(int(cfg.max_iter), float(cfg.tol_grad), float(cfg.denom_scale), int(cfg.mu_maxiter),
+                       float(cfg.tr_delta0), int(cfg.tr_cg_max), int(targets.shape[0]) if has_defl else 0,
+                       targets.data_ptr() if has_defl else None, float(cfg.deflation_sigma),
+                       float(cfg.deflation_length))
+    need = C.c_size_t(0)
+    _lib.check(L.hf_newton_workspace_size(C.byref(pb), C.byref(nc), C.byref(need)))
+    ws = _lib.workspace(need.value, dev, "newton")
+    P0d = torch.as_tensor(P0).to(dev, cd).contiguous()
+    Q = torch.empty((nk1, nk2, nb, nb), dtype=cd, device=dev)
+    p = torch.empty((nk1, nk2, nb), dtype=rd, device=dev)
+    density, fock = torch.empty_like(Q), torch.empty_like(Q)
+    m = max(int(cfg.max_iter), 1)
+    hist = np.zeros((2, m))
+    out = np.zeros(6)
+    dp = lambda a: a.ctypes.data_as(C.c_void_p)
+    _lib.check(L.hf_newton_solve(_lib.stream_ptr(dev), C.byref(pb), C.byref(nc), P0d.data_ptr(), Q.data_ptr(),
+                                 p.data_ptr(), density.data_ptr(), fock.data_ptr(), dp(hist[0]), dp(hist[1]), dp(out),
+                                 ws.data_ptr(), ws.numel()))
+    out_c, out_r = kernel.dtype, kernel.real_dtype
+    hE, hG = hist[0, :int(cfg.max_iter)], hist[1, :int(cfg.max_iter)]
+    history = dict(E=torch.as_tensor(hE, dtype=out_r), grad_norm=torch.as_tensor(hG, dtype=out_r),
+                   n_builds=int(out[5]))
+    return SolveResult(Q=Q.to(out_c), p=p.to(out_r), mu=torch.tensor(float(out[0]), dtype=out_r),
+                       density=density.to(out_c), fock=fock.to(out_c),
+                       energy=torch.tensor(float(out[1]), dtype=torch.float64, device=dev),
+                       n_iter=torch.tensor(int(out[2]), dtype=torch.int32), converged=torch.tensor(out[3] != 0.0),
+                       history=history)
+
+
 def solve_newton(kernel, P0, n_electrons, cfg, fock_build_fn=None):
     from .solver import SolveResult
     dev = kernel.device
     nk1, nk2, nb = kernel.shape
+    if USE_NATIVE and fock_build_fn is None and cfg.project_fn is None and cfg.block_sizes is None and nb <= 16:
+        return _solve_newton_native(kernel, P0, n_electrons, cfg)
     cd, rd = torch.complex128, torch.float64
     h = kernel.h.to(cd).contiguous()
     w2d = kernel.w2d.to(rd).contiguous()
@@ -133,12 +211,7 @@ def solve_newton(kernel, P0, n_electrons, cfg, fock_build_fn=None):
 
     has_defl = cfg.deflation_targets is not None and float(cfg.deflation_sigma) > 0.0
     if has_defl:
-        targets = torch.as_tensor(cfg.deflation_targets).to(dev, cd)
-        if targets.ndim == 4:
-            targets = targets[None]
-        if targets.ndim != 5 or tuple(targets.shape[1:]) != (nk1, nk2, nb, nb):
-            raise ValueError("deflation_targets must have shape (n_solutions, nk1, nk2, nb, nb) matching the kernel; "
-                             f"got {tuple(targets.shape)}.")
+        targets = _deflation_targets(cfg, dev, (nk1, nk2, nb, nb))
         inv2L2 = 1.0 / (2.0 * max(float(cfg.deflation_length), 1e-12) ** 2)
         dsig = float(cfg.deflation_sigma)
 
