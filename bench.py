@@ -239,7 +239,50 @@ def run_ours(args, ws, rank, local):
 
     variants["c128_batch_1stream"] = batch_rate(1)
     variants["c128_batch_3streams"] = batch_rate(3)
-    del bP, bout
+
+    # block-diagonal exchange (build_fock with exchange_block_specs) against the full build,
+    # both timed the same way: the 12 density sets built back to back inside one CUDA graph
+    # (captured once, replayed), so host overhead is out of the comparison; densities made
+    # block-diagonal for the checked runs
+    blk = np.zeros((NB, NB), bool)
+    blk[:NB // 2, :NB // 2] = blk[NB // 2:, NB // 2:] = True
+    bPb = [x * torch.as_tensor(blk, device=dev) for x in bP]
+
+    def graph_rate(build_i, reps=4):
+        side = torch.cuda.Stream()
+        side.wait_stream(stream)
+        with torch.cuda.stream(side):
+            for i in range(12):
+                build_i(i)  # workspaces for this stream, before capture
+        torch.cuda.synchronize()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=side):
+            for i in range(12):
+                build_i(i)
+        graph.replay()
+        torch.cuda.synchronize()
+        eb0, eb1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        eb0.record(stream)
+        for _ in range(reps):
+            graph.replay()
+        eb1.record(stream)
+        torch.cuda.synchronize()
+        del graph
+        return 1e3 * eb0.elapsed_time(eb1) / (12 * reps)
+
+    us_full = graph_rate(lambda i: G.build_fock(bP[i], out=bout[i], **kw))
+    variants["c128_graph_full"] = {"builds_per_s": round(1e6 / us_full, 1), "us_per_build": round(us_full, 2)}
+    half = [{"block_sizes": [NB // 2, NB // 2]}]
+    quarter = [{"block_sizes": [NB // 4] * 4}]
+    for name, dens, spec, check in (("c128_graph_blocks_2x4_forced", bP, half, False),
+                                    ("c128_graph_blocks_4x2_forced", bP, quarter, False),
+                                    ("c128_graph_blocks_2x4_checked_blockdiag", bPb, half, True),
+                                    ("c128_graph_blocks_2x4_checked_coupled", bP, half, True)):
+        us_b = graph_rate(lambda i: G.build_fock(dens[i], out=bout[i], exchange_block_specs=spec,
+                                                 exchange_check_offdiag=check, exchange_offdiag_atol=1e-9, **kw))
+        variants[name] = {"builds_per_s": round(1e6 / us_b, 1), "us_per_build": round(us_b, 2),
+                          "vs_full_build": round(us_b / us_full, 3)}
+    del bP, bout, bPb
 
     solves = run_solves(dev) if args.solves else None
     variants["solves"] = solves

@@ -95,9 +95,10 @@ int hf_fock_build(void* stream, int dtype, unsigned flags, int nk1, int nk2, int
  *  - Returns HF_ERR_WORKSPACE if the mesh needs more scratch than the array
  *    holds (hf_fock_workspace_size() > HF_FOCK_STATIC_SCRATCH_BYTES; e.g. up
  *    to 192x192 with nb = 8 in complex128).
- *  - The first call on a device looks up the array's device address; make it
- *    before any stream capture.  The array stays allocated on every device
- *    that loaded this part of the library until the process exits.
+ *  - The first call in a CUDA context looks up the array's device address
+ *    (cached under the context's unique id); make it before any stream
+ *    capture.  The array stays allocated while the context lives; after a
+ *    cudaDeviceReset the next call looks the address up again.
  *  - All calls on a device share the array: calls that may overlap on the GPU
  *    race and must be serialised by the caller. */
 #define HF_FOCK_STATIC_SCRATCH_BYTES (40u << 20)
@@ -106,6 +107,47 @@ int hf_fock_build_static_scratch(void* stream, int dtype, unsigned flags, int nk
                                  const void* HH, const void* w2d, int n_contact, const void* contact_g,
                                  const void* contact_Oi, const void* contact_Oj, void* Sigma, void* H,
                                  void* F);
+
+/* Block-diagonal exchange (utils.py:206-309, build_fock with exchange_block_specs):
+ * the same outputs as hf_fock_build except that the exchange self-energy is
+ * formed only on the in-block channels of `inblock` (HOST, nb x nb bytes,
+ * symmetric, nonzero = in-block: the channels (a, b) with a and b in one block)
+ * and is zero on the others.  Only in-block channels are transformed, so the
+ * exchange passes do (in-block channels / nb^2) of the full work; the Hartree and
+ * contact terms still see every channel of P - refP, as in fock.py:66-92.
+ * Workspace: hf_fock_blocks_workspace_size (depends on the mask).  Without
+ * HF_FOCK_EXCHANGE or with every channel in-block this is hf_fock_build.
+ *
+ * hf_block_offdiag_max: out (DEVICE, n_specs + 1 float64) = { max |P - refP|,
+ * then for each spec i the max of |P - refP| over its off-block channels }, with
+ * inblock holding n_specs masks back to back (HOST; n_specs <= 8, nb <= 32;
+ * refP may be NULL).  One pass over P, no host synchronisation: the caller
+ * reads the n_specs + 1 values once and takes the first spec whose off-block
+ * maximum is <= atol + rtol * max (utils.py:263-267); NaN propagates. */
+int hf_fock_blocks_workspace_size(int dtype, unsigned flags, int nk1, int nk2, int nb,
+                                  const unsigned char* inblock, size_t* bytes);
+int hf_fock_build_blocks(void* stream, int dtype, unsigned flags, int nk1, int nk2, int nb,
+                         const unsigned char* inblock, const void* P, const void* h, const void* VR,
+                         const void* refP, const void* HH, const void* w2d, int n_contact, const void* contact_g,
+                         const void* contact_Oi, const void* contact_Oj, void* Sigma, void* H, void* F,
+                         void* workspace, size_t workspace_bytes);
+int hf_block_offdiag_max(void* stream, int dtype, size_t nk, int nb, const void* P, const void* refP, int n_specs,
+                         const unsigned char* inblock, double* out);
+
+/* build_fock with exchange_block_specs and check_offdiag (utils.py:252-309) without a
+ * host round trip: hf_block_offdiag_max, then a one-thread kernel picks the first
+ * compatible spec (or the full build) and sets a device flag; the masked build of
+ * every spec and the full build are all queued, and the kernels of every candidate
+ * but the chosen one return at once.  inblock: n_specs (1..8) masks back to back
+ * (HOST).  chosen (DEVICE int, may be NULL) receives the spec index or -1 for the
+ * full build.  Workspace: hf_fock_block_specs_workspace_size. */
+int hf_fock_block_specs_workspace_size(int dtype, unsigned flags, int nk1, int nk2, int nb, int n_specs,
+                                       const unsigned char* inblock, size_t* bytes);
+int hf_fock_build_block_specs(void* stream, int dtype, unsigned flags, int nk1, int nk2, int nb, int n_specs,
+                              const unsigned char* inblock, double atol, double rtol, const void* P, const void* h,
+                              const void* VR, const void* refP, const void* HH, const void* w2d, int n_contact,
+                              const void* contact_g, const void* contact_Oi, const void* contact_Oj, void* Sigma,
+                              void* H, void* F, void* workspace, size_t workspace_bytes, int* chosen);
 
 /* Autotuner for the Fock-build schedule (slot plan and FFT engine per shape;
  * no counterpart in the reference, whose FFTs are XLA's).  Same arguments as

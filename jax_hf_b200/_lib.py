@@ -44,6 +44,13 @@ _SIGS = {
     "hf_fock_workspace_size": ([i32, u32, i32, i32, i32, psz], i32),
     "hf_fock_build": ([vp, i32, u32, i32, i32, i32, vp, vp, vp, vp, vp, vp, i32, vp, vp, vp,
                        vp, vp, vp, vp, sz], i32),
+    "hf_fock_blocks_workspace_size": ([i32, u32, i32, i32, i32, vp, psz], i32),
+    "hf_fock_build_blocks": ([vp, i32, u32, i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, i32, vp, vp, vp, vp, vp, vp,
+                              vp, sz], i32),
+    "hf_block_offdiag_max": ([vp, i32, sz, i32, vp, vp, i32, vp, vp], i32),
+    "hf_fock_block_specs_workspace_size": ([i32, u32, i32, i32, i32, i32, vp, psz], i32),
+    "hf_fock_build_block_specs": ([vp, i32, u32, i32, i32, i32, i32, vp, f64, f64, vp, vp, vp, vp, vp, vp, i32, vp,
+                                   vp, vp, vp, vp, vp, vp, sz, vp], i32),
     "hf_fock_autotune": ([vp, i32, u32, i32, i32, i32, vp, vp, vp, vp, vp, vp, i32, vp, vp, vp,
                           vp, vp, vp, vp, sz, i32, C.POINTER(C.c_uint), C.POINTER(C.c_float)], i32),
     "hf_fock_autotune_reset": ([], i32),

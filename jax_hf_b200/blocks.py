@@ -2,12 +2,18 @@
 
 Semantics of the reference: with ``block_specs`` the exchange is computed block by
 block for the first spec whose off-block entries satisfy
-``max|P| * mask <= atol + rtol * max|P|`` (or unconditionally with
-``check_offdiag=False``); off-block channels of Sigma are then zero, while the
-contact and Hartree terms still see the whole density.  Because exchange
-channels are independent, the block result is the CUDA exchange of the
-in-block channels of P - refP; off-block channels contribute nothing.  The
-contact term is added from the full density afterwards.
+``max|P - refP| * mask <= atol + rtol * max|P - refP|`` (or unconditionally with
+``check_offdiag=False``); off-block channels of Sigma's exchange part are then
+zero, while the Hartree and contact terms still see the whole density.
+
+On the GPU (``hf_fock_build_block_specs``): one kernel evaluates the off-block
+maxima of every spec in a single pass over P - refP, a one-thread kernel picks the
+first compatible spec and sets a device flag, and the masked build of every spec
+plus the full build are queued behind it; only the flagged candidate's kernels do
+any work, so the host never waits.  A masked build (``hf_fock_build_blocks``)
+transforms only the in-block channels, one slot group per block (two 4x4 blocks
+of nb = 8: half of the channels), and writes the off-block channels in a separate
+pass.  ``choose_spec`` is the host-side form of the same choice (one read).
 """
 
 from __future__ import annotations
@@ -85,52 +91,59 @@ def inblock_mask(kind, data, n):
     return m
 
 
+_MASKS: dict = {}
+
+
+def spec_masks(specs, n):
+    """In-block masks (uint8, (len(specs), n, n)) of normalised specs; cached per (specs, n)."""
+    key = (specs, int(n))
+    m = _MASKS.get(key)
+    if m is None:
+        m = np.stack([inblock_mask(kind, data, n) for kind, data in specs]).astype(np.uint8)
+        m = np.ascontiguousarray(m)
+        _MASKS[key] = m
+    return m
+
+
+def choose_spec(P, refP, specs, masks, *, check, atol, rtol):
+    """Index of the first spec whose off-block |P - refP| is within tolerance (utils.py:263-309),
+    or None for the full build.  One device pass and one host read for all specs."""
+    from . import _lib
+    if not check:
+        return 0
+    n = int(P.shape[-1])
+    nk = int(P.shape[0]) * int(P.shape[1])
+    refPt = None if refP is None or is_marked_zero(refP) else refP
+    out = torch.empty(len(specs) + 1, dtype=torch.float64, device=P.device)
+    _lib.check(_lib.lib().hf_block_offdiag_max(
+        _lib.stream_ptr(P.device), _lib.dtype_code(P), nk, n, P.data_ptr(), _lib.ptr(refPt), len(specs),
+        masks.ctypes.data_as(_lib.C.c_void_p), out.data_ptr()))
+    vals = out.cpu().numpy()
+    tol = float(atol) + float(rtol) * float(vals[0])
+    for i in range(len(specs)):
+        if vals[i + 1] <= tol:
+            return i
+    return None
+
+
 def build_fock_block_specs(P, *, h, VR, refP, HH, w2d, include_exchange, include_hartree,
                            exchange_hermitian_channel_packing, contact_g=None, contact_Oi=None, contact_Oj=None,
                            exchange_block_specs=None, exchange_check_offdiag=None, exchange_offdiag_atol=1e-12,
                            exchange_offdiag_rtol=0.0, project_fn=None, fft_precision=None):
-    from .fock import build_fock, _herm
+    from .fock import build_fock
     specs = normalize_block_specs(exchange_block_specs)
-    common = dict(h=h, VR=VR, HH=HH, w2d=w2d, include_hartree=include_hartree,
-                  exchange_hermitian_channel_packing=exchange_hermitian_channel_packing,
-                  fft_precision=fft_precision)
+    common = dict(h=h, VR=VR, refP=refP, HH=HH, w2d=w2d, include_hartree=include_hartree,
+                  exchange_hermitian_channel_packing=exchange_hermitian_channel_packing, contact_g=contact_g,
+                  contact_Oi=contact_Oi, contact_Oj=contact_Oj, project_fn=project_fn, fft_precision=fft_precision)
     if not specs or not include_exchange:
-        return build_fock(P, refP=refP, include_exchange=include_exchange, contact_g=contact_g,
-                          contact_Oi=contact_Oi, contact_Oj=contact_Oj, project_fn=project_fn, **common)
+        return build_fock(P, include_exchange=include_exchange, **common)
+    if len(specs) > 8:
+        raise ValueError("at most 8 block specs are supported")
     n = int(P.shape[-1])
+    masks = spec_masks(specs, n)
     check = bool(exchange_check_offdiag) if exchange_check_offdiag is not None else True
-    chosen = None
-    if check:
-        absP = P.abs()
-        tol = float(exchange_offdiag_atol) + float(exchange_offdiag_rtol) * float(absP.max())
-        for kind, data in specs:
-            off = torch.as_tensor(~inblock_mask(kind, data, n), device=P.device)
-            if float((absP * off).max()) <= tol:
-                chosen = (kind, data)
-                break
-    else:
-        chosen = specs[0]
-    if chosen is None:                                           # no compatible spec: full path
-        return build_fock(P, refP=refP, include_exchange=True, contact_g=contact_g, contact_Oi=contact_Oi,
-                          contact_Oj=contact_Oj, project_fn=project_fn, **common)
-    mask = torch.as_tensor(inblock_mask(*chosen, n), device=P.device).to(P.dtype)
-    Pm = P * mask
-    refm = None if refP is None or is_marked_zero(refP) else refP * mask
-    Sg, H, F = build_fock(Pm, refP=refm, include_exchange=True, **common)
-    if include_hartree and refm is not None:
-        pass  # the Hartree term only reads diagonal channels, which are in-block
-    has_contact = contact_g is not None and contact_Oi is not None and contact_Oj is not None and \
-        not is_marked_zero(contact_g)
-    if has_contact:
-        dP = P if refP is None or is_marked_zero(refP) else P - refP
-        rho = torch.einsum("ij,ijab->ab", w2d.to(P.dtype), dP)
-        tr = torch.einsum("tij,ji->t", contact_Oj, rho)
-        s_h = torch.einsum("t,tij->ij", contact_g.to(P.dtype) * tr, contact_Oi)
-        s_f = torch.einsum("t,tij->ij", -contact_g.to(P.dtype),
-                           torch.einsum("tik,tkl->til", torch.einsum("tij,jk->tik", contact_Oi, rho), contact_Oj))
-        sc = (s_h + s_f)[None, None]
-        Sg = Sg + sc
-        F = F + _herm(sc.expand_as(F))
-    if project_fn is not None:
-        F = _herm(torch.as_tensor(project_fn(F)).to(P.dtype))
-    return Sg, H, F
+    if not check:                                                # the first spec, unconditionally
+        return build_fock(P, include_exchange=True, _inblock=masks[0], **common)
+    # the device picks the spec (or the full build): no host round trip
+    return build_fock(P, include_exchange=True, _inblock=masks,
+                      _spec_check=(float(exchange_offdiag_atol), float(exchange_offdiag_rtol)), **common)

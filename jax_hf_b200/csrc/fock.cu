@@ -52,15 +52,62 @@ static FftPlan1D make_fft_plan(int n) {
 }
 
 // Units are transpose-closed channel sets built from 2x2 tiles; full mode pairs
-// tile (I,J) with (J,I); packing mode keeps the upper triangle only.
-static std::vector<std::vector<int>> make_units(int nb, bool packing) {
+// tile (I,J) with (J,I); packing mode keeps the upper triangle only.  With an
+// in-block mask (nb x nb, symmetric, 1 = in-block) only in-block channels enter a
+// unit, so the exchange passes never transform an off-block channel.
+static std::vector<std::vector<int>> make_units(int nb, bool packing, const unsigned char* inb = nullptr);
+
+// A block-diagonal mask (every band's in-block row is its own block: the relation is an
+// equivalence, as for block_sizes and disjoint block_indices) gets one unit per block,
+// C x C channels (upper triangle with packing), so each k-point's channels of a block
+// are read and written as whole rows of the block; blocks of more than 16 channels are
+// split into 2x2 tile pairs of their own bands.  Returns false for other masks.
+static bool block_units(int nb, bool packing, const unsigned char* inb, std::vector<std::vector<int>>& units) {
+  std::vector<unsigned> row(nb, 0u);
+  for (int a = 0; a < nb; ++a)
+    for (int b = 0; b < nb; ++b)
+      if (inb[a * nb + b]) row[a] |= 1u << b;
+  for (int a = 0; a < nb; ++a) {
+    if (!row[a]) continue;
+    if (!((row[a] >> a) & 1u)) return false;
+    for (int b = 0; b < nb; ++b)
+      if (((row[a] >> b) & 1u) && row[b] != row[a]) return false;
+  }
+  units.clear();
+  unsigned seen = 0u;
+  for (int a = 0; a < nb; ++a) {
+    if (!row[a] || (seen & row[a])) continue;
+    seen |= row[a];
+    std::vector<int> cls;
+    for (int b = 0; b < nb; ++b)
+      if ((row[a] >> b) & 1u) cls.push_back(b);
+    const int m = (int)cls.size();
+    if (m * m <= 16) {
+      std::vector<int> u;
+      for (int i = 0; i < m; ++i)
+        for (int j = packing ? i : 0; j < m; ++j) u.push_back(cls[i] * nb + cls[j]);
+      units.push_back(u);
+      continue;
+    }
+    // the tile units of an m-band problem, mapped onto the block's bands
+    for (const auto& t : make_units(m, packing)) {
+      std::vector<int> u;
+      for (int c : t) u.push_back(cls[c / m] * nb + cls[c % m]);
+      units.push_back(u);
+    }
+  }
+  return true;
+}
+
+static std::vector<std::vector<int>> make_units(int nb, bool packing, const unsigned char* inb) {
   std::vector<std::vector<int>> units;
+  if (inb && block_units(nb, packing, inb, units)) return units;
   const int T = (nb + 1) / 2;
   auto tile = [&](int I, int J, bool upper_only) {
     std::vector<int> v;
     for (int a = 2 * I; a < std::min(2 * I + 2, nb); ++a)
       for (int b = 2 * J; b < std::min(2 * J + 2, nb); ++b)
-        if (!upper_only || a <= b) v.push_back(a * nb + b);
+        if ((!upper_only || a <= b) && (!inb || inb[a * nb + b])) v.push_back(a * nb + b);
     return v;
   };
   for (int I = 0; I < T; ++I)
@@ -70,7 +117,7 @@ static std::vector<std::vector<int>> make_units(int nb, bool packing) {
         std::vector<int> t = tile(J, I, false);
         u.insert(u.end(), t.begin(), t.end());
       }
-      units.push_back(u);
+      if (!u.empty()) units.push_back(u);
     }
   return units;
 }
@@ -102,8 +149,16 @@ static size_t fock_smem_bytes(int n, int LS) {
   return (size_t)(2 * n * LS + n) * sizeof(cpx_t<FT>);
 }
 
-static int plan_slots(int nb, bool packing, int nmax, size_t celem, int max_ls, SlotPlan& out) {
-  auto units = make_units(nb, packing);
+static int plan_slots(int nb, bool packing, int nmax, size_t celem, int max_ls, SlotPlan& out,
+                      const unsigned char* inb = nullptr) {
+  auto units = make_units(nb, packing, inb);
+  if (units.empty()) {  // no channel to transform (an in-block mask without in-block channels)
+    out.LS = 16;
+    out.ngroups = 0;
+    out.chan.clear();
+    out.partner.clear();
+    return HF_OK;
+  }
   int maxu = 0, total = 0;
   for (auto& u : units) { maxu = std::max<int>(maxu, (int)u.size()); total += (int)u.size(); }
   const size_t kTwoPerSm = 113 * 1024, kOnePerSm = 227 * 1024;
@@ -127,6 +182,8 @@ static int plan_slots(int nb, bool packing, int nmax, size_t celem, int max_ls, 
   out.ngroups = (int)best_groups.size();
   out.chan.assign(out.LS * out.ngroups, -1);
   out.partner.assign(out.LS * out.ngroups, -1);
+  if (inb)  // ascending channels: each k-point's in-block runs are read and written in order
+    for (auto& grp : best_groups) std::sort(grp.begin(), grp.end());
   for (int g = 0; g < out.ngroups; ++g) {
     const auto& grp = best_groups[g];
     for (size_t s = 0; s < grp.size(); ++s) out.chan[g * out.LS + s] = (int16_t)grp[s];
@@ -390,13 +447,15 @@ struct WsLayout {
   size_t scratch = 0, rho = 0, sigc = 0, hdiag = 0, total = 0;
 };
 
-static WsLayout ws_layout(const SlotPlan& sp, int nk1, int nk2, int nb, size_t felem, bool exch) {
+// rho_slots: slots of the plan that forms the constant terms (-1: the exchange plan's)
+static WsLayout ws_layout(const SlotPlan& sp, int nk1, int nk2, int nb, size_t felem, bool exch,
+                          int rho_slots = -1) {
   WsLayout w;
   size_t off = 0;
   w.scratch = off;
   if (exch) off += align_up((size_t)sp.ngroups * sp.LS * nk1 * nk2 * felem, 256);
   w.rho = off;
-  off += align_up((size_t)nk1 * sp.ngroups * sp.LS * sizeof(double2), 256);
+  off += align_up((size_t)nk1 * (rho_slots >= 0 ? rho_slots : sp.ngroups * sp.LS) * sizeof(double2), 256);
   w.sigc = off;
   off += align_up((size_t)nb * nb * sizeof(double2), 256);
   w.hdiag = off;
@@ -441,21 +500,110 @@ static void plan_rows(int nb, SlotPlan& out) {
   }
 }
 
-static int get_plan(int dtype, unsigned flags, int nk1, int nk2, int nb, SlotPlan& sp) {
+static int get_plan(int dtype, unsigned flags, int nk1, int nk2, int nb, SlotPlan& sp,
+                    const unsigned char* inb = nullptr) {
   const bool packing = (flags & HF_FOCK_PACKING) != 0;
-  if (!packing && nb <= 8 && !(flags & (HF_FOCK_GENERIC_FFT | HF_FOCK_TILE_PLAN)) && fast_length(nk1) &&
+  if (!inb && !packing && nb <= 8 && !(flags & (HF_FOCK_GENERIC_FFT | HF_FOCK_TILE_PLAN)) && fast_length(nk1) &&
       fast_length(nk2)) {
     plan_rows(nb, sp);
     return HF_OK;
   }
   const int max_ls = (fast_length(nk1) && fast_length(nk2)) ? 16 : 32;
-  int st = plan_slots(nb, packing, std::max(nk1, nk2), fft_elem(dtype, flags), max_ls, sp);
+  int st = plan_slots(nb, packing, std::max(nk1, nk2), fft_elem(dtype, flags), max_ls, sp, inb);
   if (st != HF_OK) return fail(st, "mesh too large for the shared-memory FFT (nk1, nk2 <= 768 in complex128)");
   return HF_OK;
 }
 
+// Sigma and F on the off-block channels of an in-block mask (listed in `off`): no
+// exchange there, so Sigma = the contact constant and F = herm(h + Sigma) + the
+// Hartree diagonal, the epilogue's formula with a zero exchange term.  One thread per
+// (k, off-block channel), channels ascending within a k-point.
+struct OffBlockList {
+  int16_t ch[kMaxNb * kMaxNb];
+  int n;
+};
+
+template <typename ST>
+__global__ void k_fock_offblock(unsigned nk, int nb, const __grid_constant__ OffBlockList m, const void* hv,
+                                const double2* __restrict__ sigc, const double* __restrict__ hdiag, void* Sgv,
+                                void* Fv, const int* active) {
+  if (active && !*active) return;
+  using SC = cpx_t<ST>;
+  const SC* h = static_cast<const SC*>(hv);
+  SC* Sg = static_cast<SC*>(Sgv);
+  SC* F = static_cast<SC*>(Fv);
+  constexpr int U = 4;  // elements per thread and step, loads issued first
+  const unsigned nb2 = (unsigned)(nb * nb), n = nk * (unsigned)m.n, stride = gridDim.x * blockDim.x;
+  for (unsigned j0 = blockIdx.x * blockDim.x + threadIdx.x; j0 < n; j0 += U * stride) {
+    SC hab[U], hba[U];
+    size_t at[U];
+    int cs[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const unsigned j = j0 + u * stride;
+      const unsigned k = j < n ? j / (unsigned)m.n : 0u;
+      const int c = j < n ? m.ch[j - k * (unsigned)m.n] : 0;
+      const int a = c / nb, b = c - a * nb;
+      cs[u] = c;
+      at[u] = (size_t)k * nb2;
+      hab[u] = j < n ? h[at[u] + c] : mk<SC>(0.0, 0.0);
+      hba[u] = j < n ? h[at[u] + b * nb + a] : mk<SC>(0.0, 0.0);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (j0 + u * stride >= n) break;
+      const int c = cs[u], a = c / nb, b = c - a * nb;
+      SC sab = mk<SC>(0.0, 0.0), sba = mk<SC>(0.0, 0.0);
+      if (sigc) {
+        sab = cvt<SC>(sigc[c]);
+        sba = cvt<SC>(sigc[b * nb + a]);
+      }
+      SC f = mk<SC>(0.5 * ((double)hab[u].x + (double)hba[u].x) + 0.5 * ((double)sab.x + (double)sba.x),
+                    0.5 * ((double)hab[u].y - (double)hba[u].y) + 0.5 * ((double)sab.y - (double)sba.y));
+      if (hdiag && a == b) f.x += (ST)hdiag[a];
+      Sg[at[u] + c] = sab;
+      F[at[u] + c] = f;
+    }
+  }
+}
+
+template <typename ST>
+static int launch_consts(const FockParams& q, cudaStream_t stream) {
+  k_fock_rho_part<ST><<<dim3(q.nk1, q.ngroups), kThreads, 0, stream>>>(q);
+  HF_LAUNCH_CHECK("k_fock_rho_part");
+  k_fock_consts<ST><<<1, 256, 0, stream>>>(q);
+  HF_LAUNCH_CHECK("k_fock_consts");
+  return HF_OK;
+}
+
+// A side stream and two events per host thread and CUDA context, for forking work off the
+// caller's stream and joining it back (also inside stream capture, where the fork and
+// join become graph edges).  Per thread, so concurrent callers never share an event.
+struct ForkJoin {
+  unsigned long long ctx = 0;
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+};
+
+static int fork_join(ForkJoin** out) {
+  thread_local ForkJoin fj;
+  unsigned long long ctx = 0;
+  int st = context_id(&ctx);
+  if (st) return st;
+  if (!fj.side || fj.ctx != ctx) {  // first use in this context (a reset context's handles are gone)
+    HF_CUDA(cudaStreamCreateWithFlags(&fj.side, cudaStreamNonBlocking));
+    HF_CUDA(cudaEventCreateWithFlags(&fj.fork, cudaEventDisableTiming));
+    HF_CUDA(cudaEventCreateWithFlags(&fj.join, cudaEventDisableTiming));
+    fj.ctx = ctx;
+  }
+  *out = &fj;
+  return HF_OK;
+}
+
+// pc: the plan for the constant terms when it differs from the exchange plan (an
+// in-block mask: the Hartree and contact terms read every channel of the density).
 template <typename ST, typename FT>
-static int launch_fock(FockParams& p, cudaStream_t stream, bool need_consts) {
+static int launch_fock(FockParams& p, cudaStream_t stream, bool need_consts, const FockParams* pc = nullptr) {
   const bool exch = (p.flags & HF_FOCK_EXCHANGE) != 0;
   const size_t sm_row = fock_smem_bytes<FT>(p.nk2, p.LS);
   const size_t sm_col = fock_smem_bytes<FT>(p.nk1, p.LS);
@@ -464,11 +612,13 @@ static int launch_fock(FockParams& p, cudaStream_t stream, bool need_consts) {
   HF_SMEM_CAP(k_fock_row_inv<ST, FT>);
   dim3 grow(p.nk1, p.ngroups), gcol(p.nk2, p.ngroups);
   if (need_consts) {
-    k_fock_rho_part<ST><<<grow, kThreads, 0, stream>>>(p);
+    const FockParams& q = pc ? *pc : p;
+    k_fock_rho_part<ST><<<dim3(q.nk1, q.ngroups), kThreads, 0, stream>>>(q);
     HF_LAUNCH_CHECK("k_fock_rho_part");
-    k_fock_consts<ST><<<1, 256, 0, stream>>>(p);
+    k_fock_consts<ST><<<1, 256, 0, stream>>>(q);
     HF_LAUNCH_CHECK("k_fock_consts");
   }
+  if (p.ngroups == 0) return HF_OK;  // an in-block mask without in-block channels
   if (!(p.flags & HF_FOCK_GENERIC_FFT)) {
     bool handled = false;
     int st = pipe_fock<ST, FT>(p, stream, &handled);
@@ -562,12 +712,23 @@ extern "C" int hf_fock_build(void* stream, int dtype, unsigned flags, int nk1, i
                                  nullptr);
 }
 
-// The build with exactly these flags (no stored autotuner choice applied).
+// Workspace of a build whose exchange covers only the in-block channels of `inb`.
+static int masked_ws(int dtype, unsigned flags, int nk1, int nk2, int nb, const unsigned char* inb, SlotPlan& sp,
+                     SlotPlan& spc, WsLayout& wl) {
+  int st;
+  if ((st = get_plan(dtype, flags, nk1, nk2, nb, sp, inb))) return st;
+  if ((st = get_plan(dtype, flags & ~kEngineFlags, nk1, nk2, nb, spc))) return st;
+  wl = ws_layout(sp, nk1, nk2, nb, fft_elem(dtype, flags), true, spc.ngroups * spc.LS);
+  return HF_OK;
+}
+
+// The build with exactly these flags (no stored autotuner choice applied).  inb: an
+// in-block channel mask (nb x nb, symmetric; NULL = every channel) for the exchange.
 static int fock_build_exact(void* stream, int dtype, unsigned flags, int nk1, int nk2, int nb, const void* P,
                             const void* h, const void* VR, const void* refP, const void* HH, const void* w2d,
                             int n_contact, const void* contact_g, const void* contact_Oi,
                             const void* contact_Oj, void* Sigma, void* H, void* F, void* workspace,
-                            size_t workspace_bytes, const int* active) {
+                            size_t workspace_bytes, const int* active, const unsigned char* inb = nullptr) {
   int st = validate(dtype, flags, nk1, nk2, nb);
   if (st) return st;
   const bool exch = (flags & HF_FOCK_EXCHANGE) != 0;
@@ -578,9 +739,14 @@ static int fock_build_exact(void* stream, int dtype, unsigned flags, int nk1, in
   if (n_contact < 0) return fail(HF_ERR_INVALID, "n_contact must be >= 0");
   if (n_contact > 0 && (!contact_g || !contact_Oi || !contact_Oj || !w2d))
     return fail(HF_ERR_INVALID, "contact terms need g, O_i, O_j and w2d");
-  SlotPlan sp;
-  if ((st = get_plan(dtype, flags, nk1, nk2, nb, sp))) return st;
-  WsLayout wl = ws_layout(sp, nk1, nk2, nb, fft_elem(dtype, flags), exch);
+  SlotPlan sp, spc;
+  WsLayout wl;
+  if (inb) {
+    if ((st = masked_ws(dtype, flags, nk1, nk2, nb, inb, sp, spc, wl))) return st;
+  } else {
+    if ((st = get_plan(dtype, flags, nk1, nk2, nb, sp))) return st;
+    wl = ws_layout(sp, nk1, nk2, nb, fft_elem(dtype, flags), exch);
+  }
   if (!workspace || workspace_bytes < wl.total)
     return fail(HF_ERR_WORKSPACE, "workspace too small: need " + std::to_string(wl.total) + " bytes");
   if (reinterpret_cast<uintptr_t>(workspace) % 256 != 0)
@@ -614,9 +780,54 @@ static int fock_build_exact(void* stream, int dtype, unsigned flags, int nk1, in
     const size_t hb = (size_t)nb * nb * (dtype == HF_C128 ? sizeof(double2) : sizeof(float2));
     HF_CUDA(cudaMemsetAsync(H, 0, hb, s));
   }
-  if (dtype == HF_C64) return launch_fock<float, float>(p, s, need_consts);
-  if (flags & HF_FOCK_FFT_FP32) return launch_fock<double, float>(p, s, need_consts);
-  return launch_fock<double, double>(p, s, need_consts);
+  if (!inb) {
+    if (dtype == HF_C64) return launch_fock<float, float>(p, s, need_consts);
+    if (flags & HF_FOCK_FFT_FP32) return launch_fock<double, float>(p, s, need_consts);
+    return launch_fock<double, double>(p, s, need_consts);
+  }
+  // masked exchange: constant terms from the full plan, then the exchange passes over the
+  // in-block plan and, on a forked stream, the off-block channels (independent of the
+  // passes: both read only P's constants and h), so the off-block pass fills the SMs the
+  // passes leave idle in their last rounds
+  FockParams pc = p;
+  pc.LS = spc.LS;
+  pc.ngroups = spc.ngroups;
+  pc.rows_plan = spc.rows ? 1 : 0;
+  std::fill(pc.chan, pc.chan + kMaxSlotTable, (int16_t)-1);
+  std::copy(spc.chan.begin(), spc.chan.end(), pc.chan);
+  std::copy(spc.partner.begin(), spc.partner.end(), pc.partner);
+  if (need_consts) {
+    if (dtype == HF_C64) st = launch_consts<float>(pc, s);
+    else st = launch_consts<double>(pc, s);
+    if (st) return st;
+  }
+  ForkJoin* fj = nullptr;
+  if ((st = fork_join(&fj))) return st;
+  HF_CUDA(cudaEventRecord(fj->fork, s));
+  if (dtype == HF_C64) st = launch_fock<float, float>(p, s, false);
+  else if (flags & HF_FOCK_FFT_FP32) st = launch_fock<double, float>(p, s, false);
+  else st = launch_fock<double, double>(p, s, false);
+  if (st) return st;
+  OffBlockList m;
+  memset(&m, 0, sizeof(m));
+  for (int c = 0; c < nb * nb; ++c)
+    if (!inb[c]) m.ch[m.n++] = (int16_t)c;
+  if (m.n == 0) return HF_OK;
+  const unsigned nk = (unsigned)nk1 * (unsigned)nk2;
+  const size_t n = (size_t)nk * m.n;
+  if (n >= (1ull << 31)) return fail(HF_ERR_UNSUPPORTED, "mesh too large for the off-block pass");
+  const int blocks = (int)std::min<size_t>((n + 1023) / 1024, (size_t)148 * 8);
+  const double2* sigc = need_consts ? p.sigc : nullptr;
+  const double* hdiag = need_consts ? p.hdiag : nullptr;
+  HF_CUDA(cudaStreamWaitEvent(fj->side, fj->fork, 0));
+  if (dtype == HF_C64)
+    k_fock_offblock<float><<<blocks, 256, 0, fj->side>>>(nk, nb, m, h, sigc, hdiag, Sigma, F, active);
+  else
+    k_fock_offblock<double><<<blocks, 256, 0, fj->side>>>(nk, nb, m, h, sigc, hdiag, Sigma, F, active);
+  HF_LAUNCH_CHECK("k_fock_offblock");
+  HF_CUDA(cudaEventRecord(fj->join, fj->side));
+  HF_CUDA(cudaStreamWaitEvent(s, fj->join, 0));
+  return HF_OK;
 }
 
 int hf::fock_build_internal(void* stream, int dtype, unsigned flags, int nk1, int nk2, int nb, const void* P,
@@ -629,6 +840,132 @@ int hf::fock_build_internal(void* stream, int dtype, unsigned flags, int nk1, in
   return fock_build_exact(stream, dtype, tuned_flags(dtype, flags, nk1, nk2, nb), nk1, nk2, nb, P, h, VR, refP, HH,
                           w2d, n_contact, contact_g, contact_Oi, contact_Oj, Sigma, H, F, workspace, workspace_bytes,
                           active);
+}
+
+static int check_inblock(int nb, const unsigned char* inb) {
+  if (!inb) return fail(HF_ERR_INVALID, "inblock mask is NULL");
+  for (int a = 0; a < nb; ++a)
+    for (int b = 0; b < nb; ++b)
+      if ((inb[a * nb + b] != 0) != (inb[b * nb + a] != 0))
+        return fail(HF_ERR_INVALID, "inblock mask must be symmetric (blocks are sets of bands)");
+  return HF_OK;
+}
+
+extern "C" int hf_fock_blocks_workspace_size(int dtype, unsigned flags, int nk1, int nk2, int nb,
+                                             const unsigned char* inblock, size_t* bytes) {
+  if (!bytes) return fail(HF_ERR_INVALID, "bytes is NULL");
+  int st = validate(dtype, flags, nk1, nk2, nb);
+  if (st || (st = check_inblock(nb, inblock))) return st;
+  if (!(flags & HF_FOCK_EXCHANGE)) return hf_fock_workspace_size(dtype, flags, nk1, nk2, nb, bytes);
+  SlotPlan sp, spc;
+  WsLayout wl;
+  if ((st = masked_ws(dtype, flags & ~(unsigned)HF_FOCK_PIPE, nk1, nk2, nb, inblock, sp, spc, wl))) return st;
+  *bytes = wl.total;
+  return HF_OK;
+}
+
+extern "C" int hf_fock_build_blocks(void* stream, int dtype, unsigned flags, int nk1, int nk2, int nb,
+                                    const unsigned char* inblock, const void* P, const void* h, const void* VR,
+                                    const void* refP, const void* HH, const void* w2d, int n_contact,
+                                    const void* contact_g, const void* contact_Oi, const void* contact_Oj,
+                                    void* Sigma, void* H, void* F, void* workspace, size_t workspace_bytes) {
+  int st = validate(dtype, flags, nk1, nk2, nb);
+  if (st || (st = check_inblock(nb, inblock))) return st;
+  const bool all_in = std::all_of(inblock, inblock + nb * nb, [](unsigned char v) { return v != 0; });
+  if (!(flags & HF_FOCK_EXCHANGE) || all_in)  // nothing to leave out: the plain build
+    return hf::fock_build_internal(stream, dtype, flags, nk1, nk2, nb, P, h, VR, refP, HH, w2d, n_contact,
+                                   contact_g, contact_Oi, contact_Oj, Sigma, H, F, workspace, workspace_bytes,
+                                   nullptr);
+  return fock_build_exact(stream, dtype, flags & ~(unsigned)HF_FOCK_PIPE, nk1, nk2, nb, P, h, VR, refP, HH, w2d,
+                          n_contact, contact_g, contact_Oi, contact_Oj, Sigma, H, F, workspace, workspace_bytes,
+                          nullptr, inblock);
+}
+
+// ------------------------------------------------ block specs on the device -----
+// The first spec whose off-block maximum is within atol + rtol * max runs; flag[i] = 1
+// for it (flag[n_specs] for the full build when none is compatible, or a NaN maximum).
+__global__ void k_block_choose(int n_specs, double atol, double rtol, const double* __restrict__ maxima,
+                               int* __restrict__ flag, int* __restrict__ chosen) {
+  if (threadIdx.x != 0) return;
+  const double tol = atol + rtol * maxima[0];
+  int pick = n_specs;
+  for (int i = 0; i < n_specs; ++i)
+    if (maxima[i + 1] <= tol) {
+      pick = i;
+      break;
+    }
+  for (int i = 0; i <= n_specs; ++i) flag[i] = i == pick ? 1 : 0;
+  if (chosen) *chosen = pick < n_specs ? pick : -1;
+}
+
+constexpr size_t kSpecHead = 256;  // maxima (n_specs + 1 doubles) and flags (n_specs + 1 ints)
+
+static int block_specs_ws(int dtype, unsigned flags, int nk1, int nk2, int nb, int n_specs,
+                          const unsigned char* inblock, size_t* bytes) {
+  int st;
+  size_t most = 0;
+  if ((st = hf_fock_workspace_size(dtype, flags, nk1, nk2, nb, &most))) return st;
+  for (int i = 0; i < n_specs; ++i) {
+    size_t b = 0;
+    if ((st = hf_fock_blocks_workspace_size(dtype, flags, nk1, nk2, nb, inblock + (size_t)i * nb * nb, &b)))
+      return st;
+    most = std::max(most, b);
+  }
+  *bytes = kSpecHead + most;
+  return HF_OK;
+}
+
+extern "C" int hf_fock_block_specs_workspace_size(int dtype, unsigned flags, int nk1, int nk2, int nb, int n_specs,
+                                                  const unsigned char* inblock, size_t* bytes) {
+  if (!bytes) return fail(HF_ERR_INVALID, "bytes is NULL");
+  if (n_specs < 1 || n_specs > 8) return fail(HF_ERR_INVALID, "n_specs must be 1..8");
+  return block_specs_ws(dtype, flags & ~(unsigned)HF_FOCK_PIPE, nk1, nk2, nb, n_specs, inblock, bytes);
+}
+
+extern "C" int hf_fock_build_block_specs(void* stream, int dtype, unsigned flags, int nk1, int nk2, int nb,
+                                         int n_specs, const unsigned char* inblock, double atol, double rtol,
+                                         const void* P, const void* h, const void* VR, const void* refP,
+                                         const void* HH, const void* w2d, int n_contact, const void* contact_g,
+                                         const void* contact_Oi, const void* contact_Oj, void* Sigma, void* H,
+                                         void* F, void* workspace, size_t workspace_bytes, int* chosen) {
+  int st = validate(dtype, flags, nk1, nk2, nb);
+  if (st) return st;
+  if (n_specs < 1 || n_specs > 8) return fail(HF_ERR_INVALID, "n_specs must be 1..8");
+  if (!(flags & HF_FOCK_EXCHANGE)) return fail(HF_ERR_INVALID, "block specs need the exchange term");
+  flags &= ~(unsigned)HF_FOCK_PIPE;
+  for (int i = 0; i < n_specs; ++i)
+    if ((st = check_inblock(nb, inblock + (size_t)i * nb * nb))) return st;
+  size_t need = 0;
+  if ((st = block_specs_ws(dtype, flags, nk1, nk2, nb, n_specs, inblock, &need))) return st;
+  if (!workspace || workspace_bytes < need)
+    return fail(HF_ERR_WORKSPACE, "workspace too small: need " + std::to_string(need) + " bytes");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  unsigned char* ws = static_cast<unsigned char*>(workspace);
+  double* maxima = reinterpret_cast<double*>(ws);
+  int* flag = reinterpret_cast<int*>(ws + 128);
+  void* cand_ws = ws + kSpecHead;
+  const size_t cand_bytes = workspace_bytes - kSpecHead;
+  const bool has_ref = (flags & HF_FOCK_HAS_REFP) != 0;
+  if ((st = hf_block_offdiag_max(stream, dtype, (size_t)nk1 * nk2, nb, P, has_ref ? refP : nullptr, n_specs,
+                                 inblock, maxima)))
+    return st;
+  k_block_choose<<<1, 32, 0, s>>>(n_specs, atol, rtol, maxima, flag, chosen);
+  HF_LAUNCH_CHECK("k_block_choose");
+  if (H) {  // a candidate without constant terms leaves H to this
+    const size_t hb = (size_t)nb * nb * (dtype == HF_C128 ? sizeof(double2) : sizeof(float2));
+    HF_CUDA(cudaMemsetAsync(H, 0, hb, s));
+  }
+  // every candidate is queued; its kernels return at once unless its flag is set
+  for (int i = 0; i < n_specs; ++i) {
+    const unsigned char* m = inblock + (size_t)i * nb * nb;
+    const bool all_in = std::all_of(m, m + nb * nb, [](unsigned char v) { return v != 0; });
+    st = fock_build_exact(stream, dtype, all_in ? tuned_flags(dtype, flags, nk1, nk2, nb) : flags, nk1, nk2, nb,
+                          P, h, VR, refP, HH, w2d, n_contact, contact_g, contact_Oi, contact_Oj, Sigma, H, F,
+                          cand_ws, cand_bytes, flag + i, all_in ? nullptr : m);
+    if (st) return st;
+  }
+  return hf::fock_build_internal(stream, dtype, flags, nk1, nk2, nb, P, h, VR, refP, HH, w2d, n_contact, contact_g,
+                                 contact_Oi, contact_Oj, Sigma, H, F, cand_ws, cand_bytes, flag + n_specs);
 }
 
 extern "C" int hf_fock_autotune(void* stream, int dtype, unsigned flags, int nk1, int nk2, int nb, const void* P,

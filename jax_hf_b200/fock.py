@@ -61,12 +61,15 @@ def _real_of(dt: torch.dtype) -> torch.dtype:
     return torch.float64 if dt in (torch.complex128, torch.float64) else torch.float32
 
 
+_block_ws: dict = {}  # workspace sizes of block-spec builds, per (dtype, flags, shape, masks)
+
+
 def build_fock(P, *, h, VR, refP, HH, w2d, include_exchange: bool, include_hartree: bool,
                exchange_hermitian_channel_packing: bool, contact_g=None, contact_Oi=None,
                contact_Oj=None, exchange_block_specs=None, exchange_check_offdiag=None,
                exchange_offdiag_atol: float = 1e-12, exchange_offdiag_rtol: float = 0.0,
                project_fn=None, fft_precision=None, engine=None, hermitian_density: bool = False, out=None,
-               autotune: bool = False, autotune_reps: int = 5):
+               autotune: bool = False, autotune_reps: int = 5, _inblock=None, _spec_check=None):
     """Returns (Sigma, H, F) with F = herm(h + Sigma[P - refP] + H[P - refP]) (fock.py:18-97).
 
     Extensions (keyword-only, defaults keep the reference behaviour): ``fft_precision="fp32"``
@@ -74,6 +77,10 @@ def build_fock(P, *, h, VR, refP, HH, w2d, include_exchange: bool, include_hartr
     ``hermitian_density=True`` states that P (and refP) are Hermitian, which lets a kernel
     whose V(q) is real and symmetric in the band pair use the Hermitian channel packing
     (upper-triangle channels only) for a band-resolved V as well; ``out`` = (Sigma, H, F).
+    ``_inblock`` (internal, set by the block-spec path) is an (nb, nb) uint8 in-block mask:
+    the exchange is formed on those channels only (hf_fock_build_blocks); with
+    ``_spec_check = (atol, rtol)`` it is a stack of masks, one per spec, and the device
+    picks the first compatible one (hf_fock_build_block_specs).
     """
     h = _as_dev(h)
     dev = h.device
@@ -151,6 +158,39 @@ def build_fock(P, *, h, VR, refP, HH, w2d, include_exchange: bool, include_hartr
         H = torch.empty((1, 1, nb, nb), dtype=cdt, device=dev)
     dt = _lib.dtype_code(P)
     need = _lib.C.c_size_t(0)
+    if _inblock is not None and _spec_check is not None:
+        masks = np.ascontiguousarray(np.asarray(_inblock, dtype=np.uint8).reshape(-1, nb, nb))
+        mptr = masks.ctypes.data_as(_lib.C.c_void_p)
+        ns = int(masks.shape[0])
+        key = ("specs", dt, flags, nk1, nk2, nb, masks.tobytes())
+        if key not in _block_ws:
+            _lib.check(_lib.lib().hf_fock_block_specs_workspace_size(dt, flags, nk1, nk2, nb, ns, mptr,
+                                                                     _lib.C.byref(need)))
+            _block_ws[key] = int(need.value)
+        ws = _lib.workspace(_block_ws[key], dev, "fock")
+        _lib.check(_lib.lib().hf_fock_build_block_specs(
+            _lib.stream_ptr(dev), dt, flags, nk1, nk2, nb, ns, mptr, float(_spec_check[0]), float(_spec_check[1]),
+            P.data_ptr(), h.data_ptr(), _lib.ptr(VRt), _lib.ptr(refPt), _lib.ptr(HHt), _lib.ptr(w2dt), n_contact,
+            _lib.ptr(cg), _lib.ptr(cOi), _lib.ptr(cOj), Sigma.data_ptr(), H.data_ptr(), F.data_ptr(), ws.data_ptr(),
+            ws.numel(), None))
+        if project_fn is not None:
+            F = _herm(torch.as_tensor(project_fn(F)).to(cdt))
+        return Sigma, H, F
+    if _inblock is not None:
+        mask = np.ascontiguousarray(np.asarray(_inblock, dtype=np.uint8).reshape(nb, nb))
+        mptr = mask.ctypes.data_as(_lib.C.c_void_p)
+        key = ("mask", dt, flags, nk1, nk2, nb, mask.tobytes())
+        if key not in _block_ws:
+            _lib.check(_lib.lib().hf_fock_blocks_workspace_size(dt, flags, nk1, nk2, nb, mptr, _lib.C.byref(need)))
+            _block_ws[key] = int(need.value)
+        ws = _lib.workspace(_block_ws[key], dev, "fock")
+        _lib.check(_lib.lib().hf_fock_build_blocks(
+            _lib.stream_ptr(dev), dt, flags, nk1, nk2, nb, mptr, P.data_ptr(), h.data_ptr(), _lib.ptr(VRt),
+            _lib.ptr(refPt), _lib.ptr(HHt), _lib.ptr(w2dt), n_contact, _lib.ptr(cg), _lib.ptr(cOi), _lib.ptr(cOj),
+            Sigma.data_ptr(), H.data_ptr(), F.data_ptr(), ws.data_ptr(), ws.numel()))
+        if project_fn is not None:
+            F = _herm(torch.as_tensor(project_fn(F)).to(cdt))
+        return Sigma, H, F
     _lib.check(_lib.lib().hf_fock_workspace_size(dt, flags, nk1, nk2, nb, _lib.C.byref(need)))
     ws = _lib.workspace(need.value, dev, "fock")
     args = (_lib.stream_ptr(dev), dt, flags, nk1, nk2, nb, P.data_ptr(), h.data_ptr(), _lib.ptr(VRt),
