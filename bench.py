@@ -429,6 +429,17 @@ def run_solves(dev):
                      "rel_dE_vs_oracle_reference_cg": rel(r.energy, o2["reference_algorithm"]["energy"])}
         if name == "mixed":
             cg2[name]["polish_iterations"] = int(r.history["polish_iterations"])
+    # the same problem through SCF-DIIS (Newton mu, warm eigh), FP64 and mixed: both end at the
+    # self-consistent fixed point, which the CG's plateau stop misses by 1.5e-8
+    fast2 = dict(acceleration="diis", density_tol=1e-8, comm_tol=1e-7, max_iter=300, mu_method="newton",
+                 warm_eigh=True)
+    for name, cfg in (("fp64_scf", SCFConfig(**fast2)), ("mixed_scf", SCFConfig(**fast2, fp32_exchange=True))):
+        for _ in range(3):
+            solve_scf(K2, P02, p2.n_electrons, config=cfg)
+        r, ms = median_run(lambda: solve_scf(K2, P02, p2.n_electrons, config=cfg), 7)
+        cg2[name] = {"solves_per_s": round(1e3 / ms, 2), "ms_per_solve": round(ms, 2),
+                     "iterations": int(r.iterations), "converged": bool(r.converged), "energy": float(r.energy),
+                     "rel_dE_vs_oracle_fixed_point": rel(r.energy, o2["fixed_point_energy"])}
     out["cg_144x144_nb8"] = cg2
     # density scan: 64 solves
     probs = S.density_scan(64)
@@ -463,6 +474,7 @@ def run_solves(dev):
         solve_scf(K, P0, ne, config=ref_scf)
     solve_batch(Ks, P0s, nes, config=c64, lanes=16)
     solve_scf_batch(Ks, P0s, nes, config=mixed_scf, workers=8)
+    solve_scf_batch(Ks, P0s, nes, config=SCFConfig(**fast), workers=8)
     solve_batch(Ks[:16], P0s[:16], nes[:16], config=mixed_cg, lanes=16)
     scan = {"n_solves": len(probs), "oracle": "tests/golden/scan64_oracle.json (fixed point: oracle SCF-DIIS to 1e-11)"}
     t_cg, E_cg = one_by_one(lambda K, P0, ne: solve(K, P0, ne, config=c64))
@@ -477,10 +489,19 @@ def run_solves(dev):
         "solves_per_s": round(64 / (sum(t_scf) / 1e3), 2), "total_ms": round(sum(t_scf), 2),
         "p50_ms": round(float(np.percentile(t_scf, 50)), 2), "p99_ms": round(float(np.percentile(t_scf, 99)), 2),
         **errors(E_scf)}
+    fp64_fast = SCFConfig(**fast)
+    t_fs, E_fs = one_by_one(lambda K, P0, ne: solve_scf(K, P0, ne, config=fp64_fast))
+    scan["fp64_fast_scf_solve_by_solve"] = {
+        "solver": "SCF-DIIS, FP64 throughout, the mixed solver's steps (Newton mu, warm eigh), density_tol 1e-8",
+        "solves_per_s": round(64 / (sum(t_fs) / 1e3), 2), "total_ms": round(sum(t_fs), 2),
+        "p50_ms": round(float(np.percentile(t_fs, 50)), 2), "p99_ms": round(float(np.percentile(t_fs, 99)), 2),
+        **errors(E_fs)}
     legs = (("fp64_batched", "CG, tol_E 1e-9, 16 streams",
              lambda: solve_batch(Ks, P0s, nes, config=c64, lanes=16, return_times=True)),
             ("mixed_batched", "SCF-DIIS, FP32 exchange until density residual 1e-5 then FP64, Newton mu, warm eigh, "
              "8 streams", lambda: solve_scf_batch(Ks, P0s, nes, config=mixed_scf, workers=8, return_times=True)),
+            ("fp64_fast_scf_batched", "SCF-DIIS, FP64 throughout, Newton mu, warm eigh, 8 streams",
+             lambda: solve_scf_batch(Ks, P0s, nes, config=fp64_fast, workers=8, return_times=True)),
             ("mixed_cg_polish_batched", "FP32-exchange CG to tol_E 1e-6, then FP64 SCF-DIIS polish, 16 streams",
              lambda: solve_batch(Ks, P0s, nes, config=mixed_cg, lanes=16, return_times=True)))
     for name, desc, fn in legs:
@@ -490,6 +511,7 @@ def run_solves(dev):
                       "all_converged": bool(all(bool(r.converged) for r in rb)),
                       "speedup_vs_fp64_solve_by_solve": round(sum(t_cg) / ms, 3),
                       "speedup_vs_fp64_scf_solve_by_solve": round(sum(t_scf) / ms, 3),
+                      "speedup_vs_fp64_fast_scf_solve_by_solve": round(sum(t_fs) / ms, 3),
                       **errors([float(r.energy) for r in rb])}
     out["density_scan_64"] = scan
     out["gradients_96x96_nb4"] = run_gradients(dev, ev_time, base["newton_96x96_nb4"])

@@ -187,6 +187,56 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_cgr_density(CgArgs a, int fo
   }
 }
 
+// P = herm(Q diag(p) Q^H) from given occupations (hf_density_from_Qp for complex128,
+// nb <= 8): the density step of k_cgr_density without the Fermi function
+template <int NB>
+__global__ void __launch_bounds__(32 * kRowWarps) k_rows_density(int nk, const double2* __restrict__ Q,
+                                                                 const double* __restrict__ p,
+                                                                 double2* __restrict__ P) {
+  using RG = RowGroup<NB>;
+  constexpr int G = RG::G, KPW = RG::KPW, LP = RG::LP, MAT = RG::MAT;
+  __shared__ double2 st[kRowWarps][KPW][2 * MAT];
+  __shared__ double spv[kRowWarps][KPW][NB];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, g = lane / G, c = lane % G;
+  double2* SQ = st[w][g];
+  double2* SX = SQ + MAT;
+  double* SPv = spv[w][g];
+  for (int kb = (blockIdx.x * kRowWarps + w) * KPW; kb < nk; kb += gridDim.x * kRowWarps * KPW) {
+    const int k = kb + g;
+    const bool on = k < nk && c < NB;
+    const size_t base = (size_t)k * NB * NB + c;
+    if (on) {
+#pragma unroll
+      for (int r = 0; r < NB; ++r) SQ[r * LP + c] = Q[base + (size_t)r * NB];
+      SPv[c] = p[(size_t)k * NB + c];
+    }
+    __syncwarp();
+    double2 x[NB];
+    if (on) {  // X[r][c] = sum_n Q[r][n] p_n conj(Q[c][n])
+      double2 cq[NB];
+#pragma unroll
+      for (int n = 0; n < NB; ++n) cq[n] = cscale(conj(SQ[c * LP + n]), SPv[n]);
+#pragma unroll
+      for (int r = 0; r < NB; ++r) {
+        double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int n = 0; n < NB; ++n) acc = cfma(SQ[r * LP + n], cq[n], acc);
+        x[r] = acc;
+        SX[r * LP + c] = acc;
+      }
+    }
+    __syncwarp();
+    if (on) {
+#pragma unroll
+      for (int r = 0; r < NB; ++r) {
+        const double2 y = SX[c * LP + r];  // X[c][r]
+        P[base + (size_t)r * NB] = make_double2(0.5 * (x[r].x + y.x), 0.5 * (x[r].y - y.y));
+      }
+    }
+    __syncwarp();
+  }
+}
+
 // ----------------------------------- grad1: Ft, eps, G, g_p and four norms ---
 template <int NB>
 __global__ void __launch_bounds__(32 * kRowWarps) k_cgr_grad1(CgArgs a) {

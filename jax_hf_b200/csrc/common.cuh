@@ -16,6 +16,8 @@ int fail(int status, const std::string& msg);
 int cuda_check(cudaError_t e, const char* what);
 int allow_max_dynamic_smem(const void* fn);
 int context_id(unsigned long long* id);
+// P = herm(Q diag(p) Q^H), complex128, nb <= 8, lane-per-column kernel (solver_cg.cu)
+int rows_density(void* stream, int nk, int nb, const void* Q, const double* p, void* P);
 int symbol_address(const void* symbol, void** out);
 
 #define HF_SMEM_CAP(...)                                              \

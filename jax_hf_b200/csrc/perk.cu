@@ -244,6 +244,8 @@ extern "C" int hf_density_from_Qp(void* stream, int dtype, int batch, int nb, co
   if (st) return st;
   if (batch == 0) return HF_OK;
   if (!Q || !p || !P) return fail(HF_ERR_INVALID, "NULL argument");
+  // complex128 with nb <= 8: a group of lanes per k-point, one matrix column per lane
+  if (dtype == HF_C128 && nb <= 8) return hf::rows_density(stream, batch, nb, Q, static_cast<const double*>(p), P);
   Launch L = warp_launch(batch, 2 * nb * nb + nb);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (dtype == HF_C128) {

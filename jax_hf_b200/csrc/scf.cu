@@ -242,8 +242,9 @@ extern "C" int hf_scf_solve(void* stream, const hf_cg_problem* pb, const hf_scf_
     HF_CUDA(cudaMemsetAsync(S.at<void>(kFHIST), 0, (size_t)nh * qbytes, s));
   }
   std::vector<double> hv(kSCoeff + 8, 0.0);
-  // nh > 6: B is kept here between iterations and one row (the replaced slot's) is refreshed per step
-  std::vector<double> Bkeep(diis && nh > 6 ? (size_t)nh * nh : 0, 0.0);
+  // B is kept here between iterations and only the replaced slot's row is refreshed per step
+  // (hf_gram_row; each entry bit-identical to the full hf_gram's)
+  std::vector<double> Bkeep(diis ? (size_t)nh * nh : 0, 0.0);
   int k = 0, base = 0, switch_iter = -1;  // base: first iteration of the current DIIS history
   bool converged = false;
   double d_prev = INFINITY;
@@ -272,11 +273,7 @@ extern "C" int hf_scf_solve(void* stream, const hf_cg_problem* pb, const hf_scf_
     if (diis) {
       HF_CUDA(cudaMemcpyAsync(S.at<unsigned char>(kFHIST) + (size_t)(kd % nh) * qbytes, F, qbytes,
                               cudaMemcpyDeviceToDevice, s));
-      if (nh <= 6) {
-        if ((st = hf_gram(s, nh, nq, nk, nb, S.at<void>(kRH), w2d, sc + kSGram, ops))) return st;
-      } else if ((st = hf_gram_row(s, nh, kd % nh, nq, nk, nb, S.at<void>(kRH), w2d, sc + kSGram, ops))) {
-        return st;
-      }
+      if ((st = hf_gram_row(s, nh, kd % nh, nq, nk, nb, S.at<void>(kRH), w2d, sc + kSGram, ops))) return st;
     }
     if ((st = S.read(hv.data(), sc, kSCoeff))) return st;
     const double E_host = hv[kSE];
@@ -286,16 +283,9 @@ extern "C" int hf_scf_solve(void* stream, const hf_cg_problem* pb, const hf_scf_
     void* updated = S.at<void>(kUPD);
     if (diis) {
       // B_ij = sum_k w Re tr(R_i^H R_j) over every history slot (zeros where unused)
-      std::vector<double> B((size_t)nh * nh, 0.0);
-      if (nh <= 6) {
-        int q = 0;
-        for (int i = 0; i < nh; ++i)
-          for (int j = i; j < nh; ++j, ++q) B[i * nh + j] = B[j * nh + i] = hv[kSGram + q];
-      } else {
-        const int i = kd % nh;
-        for (int j = 0; j < nh; ++j) Bkeep[(size_t)i * nh + j] = Bkeep[(size_t)j * nh + i] = hv[kSGram + j];
-        B = Bkeep;
-      }
+      const int slot = kd % nh;
+      for (int j = 0; j < nh; ++j) Bkeep[(size_t)slot * nh + j] = Bkeep[(size_t)j * nh + slot] = hv[kSGram + j];
+      const std::vector<double>& B = Bkeep;
       double bmax = 0.0;
       for (double v : B) bmax = std::fmax(bmax, std::fabs(v));
       bmax = std::fmax(bmax, 1e-30);

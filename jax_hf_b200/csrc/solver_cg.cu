@@ -844,6 +844,26 @@ static int cg_eig(CgRun& r, cudaStream_t s, const double2* A, int rotate) {
 }
 
 template <int NB>
+static int rows_density_launch(cudaStream_t s, int nk, const double2* Q, const double* p, double2* P) {
+  k_rows_density<NB><<<row_blocks(nk, RowGroup<NB>::KPW), 32 * kRowWarps, 0, s>>>(nk, Q, p, P);
+  HF_LAUNCH_CHECK("k_rows_density");
+  return HF_OK;
+}
+
+int rows_density(void* stream, int nk, int nb, const void* Q, const double* p, void* P) {
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  auto q = static_cast<const double2*>(Q);
+  auto o = static_cast<double2*>(P);
+  switch (nb) {
+#define HF_NB_CASE(N) case N: return rows_density_launch<N>(s, nk, q, p, o);
+    HF_NB_CASE(1) HF_NB_CASE(2) HF_NB_CASE(3) HF_NB_CASE(4) HF_NB_CASE(5) HF_NB_CASE(6) HF_NB_CASE(7) HF_NB_CASE(8)
+#undef HF_NB_CASE
+    default: break;
+  }
+  return fail(HF_ERR_UNSUPPORTED, "rows_density: nb > 8");
+}
+
+template <int NB>
 static int eig_cols_launch(cudaStream_t s, int nk, const double2* A, const double2* Qin, double2* Qout,
                            double* eps) {
   const int per_block = kEigWarps * RowGroup<NB>::KPW;

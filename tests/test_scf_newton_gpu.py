@@ -134,7 +134,9 @@ def test_native_scf_driver_matches_python_loop(cuda, monkeypatch, name, model, n
     np.testing.assert_allclose(a.history["density_residual"][:n], b.history["density_residual"][:n],
                                rtol=1e-9, atol=1e-14)
     assert abs(float(a.energy) - float(b.energy)) <= 1e-10 * max(1.0, abs(float(b.energy)))
-    assert (a.density_matrix - b.density_matrix).abs().max().item() < 1e-6
+    # the two runs may stop a few DIIS iterations apart, so their densities agree to the scale of
+    # the stopping tolerance (density_tol <= 1e-6 here), as in the oracle comparison above
+    assert (a.density_matrix - b.density_matrix).abs().max().item() < 1e-5
     assert a.message.split()[0] == b.message.split()[0]
 
 
