@@ -504,6 +504,25 @@ def run_solves(dev):
              lambda: solve_scf_batch(Ks, P0s, nes, config=fp64_fast, workers=8, return_times=True)),
             ("mixed_cg_polish_batched", "FP32-exchange CG to tol_E 1e-6, then FP64 SCF-DIIS polish, 16 streams",
              lambda: solve_batch(Ks, P0s, nes, config=mixed_cg, lanes=16, return_times=True)))
+    # the FP64 CG batch as one CUDA graph (device-side loops), captured once and launched
+    from jax_hf_b200.solver import ScanGraph
+    import time as _time
+    t_b = _time.perf_counter()
+    sg = ScanGraph(Ks, P0s, nes, config=c64)
+    build_ms = (_time.perf_counter() - t_b) * 1e3
+    sg.run()
+    (rg, tg), ms_g = median_run(lambda: sg.run(return_times=True), 3)
+    scan["fp64_graph_batched"] = {
+        "solver": "CG, tol_E 1e-9, the whole batch as one CUDA graph (conditional WHILE node per solve), "
+                  "captured once, launched per run", "solves_per_s": round(64 / (ms_g / 1e3), 2),
+        "total_ms": round(ms_g, 2), "graph_build_ms_host_once": round(build_ms, 1),
+        "p50_ms": round(float(np.percentile(tg, 50)), 2), "p99_ms": round(float(np.percentile(tg, 99)), 2),
+        "all_converged": bool(all(bool(r.converged) for r in rg)),
+        "speedup_vs_fp64_solve_by_solve": round(sum(t_cg) / ms_g, 3),
+        "max_abs_dE_vs_oracle_reference_cg": float(np.abs(np.asarray([float(r.energy) for r in rg]) - Ecg).max()),
+        **errors([float(r.energy) for r in rg])}
+    sg.close()
+    del rg
     for name, desc, fn in legs:
         (rb, tb), ms = median_run(fn, 3)
         scan[name] = {"solver": desc, "solves_per_s": round(64 / (ms / 1e3), 2), "total_ms": round(ms, 2),

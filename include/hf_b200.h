@@ -543,6 +543,26 @@ int hf_cg_batch_workspace_size(const hf_cg_batch_item* items, int n_items, const
                                size_t* bytes_per_lane);
 int hf_cg_solve_batch(void* stream, const hf_cg_batch_item* items, int n_items, const hf_cg_config* config,
                       int n_lanes, void* workspace, size_t bytes_per_lane, double* solve_ms);
+/* The same batch as ONE CUDA graph, built and launched once: every solve is a branch
+ * init -> iteration loop(s) -> finalize whose loops are conditional WHILE nodes, their
+ * condition set on the device after every iteration, so nothing returns to the host
+ * until the last solve ends.  All solves run at once: the workspace holds n_items
+ * blocks of bytes_per_item (hf_cg_batch_workspace_size), one per solve.  Results equal
+ * hf_cg_solve_batch's, except that the loop tests run after every iteration instead of
+ * every `chunk` iterations (a mixed-precision solve that reaches half its iteration
+ * budget in the FP32 phase switches at exactly max_iter / 2).  Extension. */
+int hf_cg_solve_batch_graph(void* stream, const hf_cg_batch_item* items, int n_items, const hf_cg_config* config,
+                            void* workspace, size_t bytes_per_item, double* solve_ms);
+/* The same in three steps, for a scan run more than once: _create captures and
+ * instantiates the graph (host work, no GPU work; the items' pointers are baked in),
+ * _launch runs it after the work queued on `stream` and makes `stream` wait for it
+ * (solve_ms, may be NULL: waits and fills each solve's time), _destroy frees it
+ * (after waiting for a launch in flight).  Between launches the caller may write new
+ * starting densities into the items' P0 buffers. */
+int hf_cg_batch_graph_create(const hf_cg_batch_item* items, int n_items, const hf_cg_config* config, void* workspace,
+                             size_t bytes_per_item, void** handle);
+int hf_cg_batch_graph_launch(void* handle, void* stream, double* solve_ms);
+int hf_cg_batch_graph_destroy(void* handle);
 
 #ifdef __cplusplus
 }

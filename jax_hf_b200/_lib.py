@@ -106,6 +106,10 @@ _SIGS = {
     "hf_free_energy_vjp": ([vp, i32, i32, i32, vp, vp, f64, f64, vp], i32),
     "hf_fourier_coeffs": ([vp, i32, i32, i32, vp, vp, i32, vp, vp], i32),
     "hf_cg_solve_batch": ([vp, vp, i32, vp, i32, vp, sz, vp], i32),
+    "hf_cg_solve_batch_graph": ([vp, vp, i32, vp, vp, sz, vp], i32),
+    "hf_cg_batch_graph_create": ([vp, i32, vp, vp, sz, vp], i32),
+    "hf_cg_batch_graph_launch": ([vp, vp, vp], i32),
+    "hf_cg_batch_graph_destroy": ([vp], i32),
 }
 
 

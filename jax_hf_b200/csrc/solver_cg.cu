@@ -39,6 +39,7 @@ struct CgScalars {
   int k, active, accepted, converged, k_base;
   int first_ok;  // the first line-search trial was accepted: Q U(tau0) and eps are already formed
   int qsel;      // row path: the current Q is Vd (1) or the caller's Q buffer (0)
+  int switched_at;  // whole-batch graph: iteration of the FP32 -> FP64 switch (-1: none)
   double mu, E, E_prev, dE, grad_norm;
   double lam, pr_den, beta, tau0, tau_final, Omega0, E_fin;
 };
@@ -663,8 +664,10 @@ __global__ void k_cg_rearm(CgArgs a) {
   s->active = s->k < a.max_iter ? 1 : 0;
 }
 
+// switched_at == -2: the switch iteration recorded on the device (whole-batch graph)
 __global__ void k_cg_converged(CgArgs a, int switched_at, double* __restrict__ out) {
   CgScalars* s = a.sc;
+  if (switched_at == -2) switched_at = s->switched_at;
   s->converged = a.tol_grad > 0.0 ? (s->grad_norm <= a.tol_grad) : (s->k < a.max_iter);
   out[0] = s->mu;
   out[1] = s->E_fin;
@@ -674,6 +677,28 @@ __global__ void k_cg_converged(CgArgs a, int switched_at, double* __restrict__ o
   out[5] = (double)switched_at;
   out[6] = 0.0;
   out[7] = 0.0;
+}
+
+// ---- whole-batch graph: device-side loop control (conditional WHILE nodes) ----
+__global__ void k_cg_graph_begin(CgArgs a) { a.sc->switched_at = -1; }
+
+// the condition of a loop over iterations: go on while the solve is active, its energy
+// finite and its iteration count below the phase's limit (the host loop's tests)
+__global__ void k_cg_graph_cond(cudaGraphConditionalHandle h, CgArgs a, int k_limit) {
+  const CgScalars* s = a.sc;
+  cudaGraphSetConditional(h, (s->active && isfinite(s->E) && s->k < k_limit) ? 1u : 0u);
+}
+
+// between the FP32 and the FP64 loops: the host driver's switch (CgSolver::advance)
+__global__ void k_cg_graph_switch(CgArgs a) {
+  CgScalars* s = a.sc;
+  if (isfinite(s->E) && s->k < a.max_iter) {
+    s->switched_at = s->k;
+    s->k_base = s->k;
+    s->active = 1;
+  } else {
+    s->active = 0;
+  }
 }
 
 // ============================================================ host driver ===
@@ -950,6 +975,8 @@ struct CgSolver {
   int setup(const hf_cg_problem* pb_, const hf_cg_config* cf_, void* Q, void* p, void* density, void* fock,
             double* hist_E, double* hist_grad, double* scalars_out_, void* workspace, cudaStream_t s_,
             CgScalars* host_slot);
+  int init_ops(const void* P0);
+  int finalize_ops(bool device_switch);
   int start(const void* P0);
   int launch_chunk();
   int advance(bool* finished);
@@ -1061,6 +1088,12 @@ int CgSolver::setup(const hf_cg_problem* pb_, const hf_cg_config* cf_, void* Q, 
 }
 
 int CgSolver::start(const void* P0) {
+  const int st = init_ops(P0);
+  if (st) return st;
+  return cf->max_iter > 0 ? launch_chunk() : launch_finalize();
+}
+
+int CgSolver::init_ops(const void* P0) {
   CgArgs& a = r.a;
   const int nb = pb->nb, nb2 = nb * nb;
   int st;
@@ -1073,8 +1106,7 @@ int CgSolver::start(const void* P0) {
   HF_LAUNCH_CHECK("k_cg_init");
   if ((st = cg_fock(r, s, false, nullptr))) return st;
   if ((st = cg_eig(r, s, a.F, 0))) return st;
-  if ((st = cg_mu(r, s, cf->mu_maxiter, nullptr))) return st;
-  return cf->max_iter > 0 ? launch_chunk() : launch_finalize();
+  return cg_mu(r, s, cf->mu_maxiter, nullptr);
 }
 
 // One iteration captured into a CUDA graph per precision phase (no host
@@ -1140,10 +1172,16 @@ int CgSolver::advance(bool* finished) {
 
 // ---- finalize (solver.py:613-648) ----
 int CgSolver::launch_finalize() {
-  CgArgs& a = r.a;
-  const int nb = pb->nb, nb2 = nb * nb;
-  int st;
   finalizing = true;
+  const int st = finalize_ops(false);
+  if (st) return st;
+  HF_CUDA(cudaMemcpyAsync(hs, r.a.sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, s));
+  return HF_OK;
+}
+
+int CgSolver::finalize_ops(bool device_switch) {
+  CgArgs& a = r.a;
+  int st;
   if ((st = cg_density(r, s, 1))) return st;
   if ((st = cg_project(r, s))) return st;
   if ((st = cg_fock(r, s, false, nullptr))) return st;
@@ -1155,9 +1193,8 @@ int CgSolver::launch_finalize() {
   if ((st = cg_project(r, s))) return st;
   if ((st = cg_fock(r, s, false, nullptr))) return st;
   if ((st = cg_energy(r, s, &a.sc->E_fin, nullptr))) return st;
-  k_cg_converged<<<1, 1, 0, s>>>(a, switched_at, scalars_out);
+  k_cg_converged<<<1, 1, 0, s>>>(a, device_switch ? -2 : switched_at, scalars_out);
   HF_LAUNCH_CHECK("k_cg_converged");
-  HF_CUDA(cudaMemcpyAsync(hs, a.sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, s));
   return HF_OK;
 }
 
@@ -1363,4 +1400,202 @@ extern "C" int hf_eigh_warm(void* stream, int nk, int nb, const void* A, const v
     default: break;
   }
   return fail(HF_ERR_UNSUPPORTED, "hf_eigh_warm: nb > 8");
+}
+
+// The whole batch as ONE CUDA graph: every solve is an independent branch
+//   init -> [WHILE: FP32 iteration] -> [switch] -> WHILE: FP64 iteration -> finalize
+// whose loops are conditional WHILE nodes: the last kernel of an iteration body sets
+// the loop's condition on the device (k_cg_graph_cond), so no host round trip happens
+// between the launch and the end of the last solve.  Each solve has its own workspace
+// (bytes_per_item from hf_cg_batch_workspace_size, n_items of them back to back), so
+// all solves may run at once; the GPU interleaves the branches' kernels.  Per-solve
+// times come from event nodes at each branch's ends.  Loop tests run after every
+// iteration (the stream driver tests every `chunk` iterations), so a solve whose FP32
+// phase ends at the half-budget limit may switch a few iterations earlier than there.
+// The graph reads P0 and writes the outputs through the items' pointers, so a built
+// batch can be launched again after new starting densities are written to the P0s.
+struct CgBatchGraph {
+  int n = 0;
+  cudaGraph_t G = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t run = nullptr;  // the stream the graph runs on, ordered after the caller's
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  std::vector<cudaEvent_t> t0, t1;
+  ~CgBatchGraph() {
+    if (run) cudaStreamSynchronize(run);  // never free a graph that may still run
+    if (exec) cudaGraphExecDestroy(exec);
+    if (run) cudaStreamDestroy(run);
+    if (ev_in) cudaEventDestroy(ev_in);
+    if (ev_out) cudaEventDestroy(ev_out);
+    if (G) cudaGraphDestroy(G);
+    for (auto e : t0)
+      if (e) cudaEventDestroy(e);
+    for (auto e : t1)
+      if (e) cudaEventDestroy(e);
+  }
+};
+
+extern "C" int hf_cg_batch_graph_create(const hf_cg_batch_item* items, int n_items, const hf_cg_config* cf,
+                                        void* workspace, size_t bytes_per_item, void** handle) {
+  if (!items || n_items < 1 || !cf || !workspace || !handle) return fail(HF_ERR_INVALID, "bad batch arguments");
+  *handle = nullptr;
+  if (cf->fock_cb || cf->project_cb) return fail(HF_ERR_INVALID, "the batched CG driver takes no host callbacks");
+  size_t need = 0;
+  int st = hf_cg_batch_workspace_size(items, n_items, cf, &need);
+  if (st) return st;
+  if (bytes_per_item < need)
+    return fail(HF_ERR_WORKSPACE, "CG batch workspace too small: need " + std::to_string(need) + " per solve");
+  for (int i = 0; i < n_items; ++i) {
+    const hf_cg_batch_item& it = items[i];
+    if (!it.P0 || !it.Q || !it.p || !it.density || !it.fock || !it.scalars_out)
+      return fail(HF_ERR_INVALID, "NULL argument in batch item " + std::to_string(i));
+  }
+  auto* bg = new CgBatchGraph();
+  bg->n = n_items;
+  bg->t0.assign(n_items, nullptr);
+  bg->t1.assign(n_items, nullptr);
+  cudaStream_t cap = nullptr;
+  CgScalars unused{};
+  auto capture_into = [&](cudaGraph_t g, const std::vector<cudaGraphNode_t>& deps) -> int {
+    HF_CUDA(cudaStreamBeginCaptureToGraph(cap, g, deps.empty() ? nullptr : deps.data(), nullptr, deps.size(),
+                                          cudaStreamCaptureModeThreadLocal));
+    return HF_OK;
+  };
+  // ends a capture and returns its terminal nodes (the next stage's dependencies)
+  auto end_capture = [&](std::vector<cudaGraphNode_t>* tail) -> int {
+    if (tail) {
+      cudaStreamCaptureStatus cs;
+      const cudaGraphNode_t* d = nullptr;
+      size_t nd = 0;
+      HF_CUDA(cudaStreamGetCaptureInfo(cap, &cs, nullptr, nullptr, &d, &nd));
+      tail->assign(d, d + nd);
+    }
+    cudaGraph_t g = nullptr;
+    HF_CUDA(cudaStreamEndCapture(cap, &g));
+    return HF_OK;
+  };
+  auto build = [&]() -> int {
+    int e;
+    HF_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    HF_CUDA(cudaGraphCreate(&bg->G, 0));
+    cudaGraph_t G = bg->G;
+    for (int i = 0; i < n_items; ++i) {
+      const hf_cg_batch_item& it = items[i];
+      CgSolver v;
+      char* ws = static_cast<char*>(workspace) + (size_t)i * bytes_per_item;
+      if ((e = v.setup(&it.problem, cf, it.Q, it.p, it.density, it.fock, it.hist_E, it.hist_grad, it.scalars_out,
+                       ws, cap, &unused)))
+        return e;
+      HF_CUDA(cudaEventCreate(&bg->t0[i]));
+      HF_CUDA(cudaEventCreate(&bg->t1[i]));
+      std::vector<cudaGraphNode_t> tail;
+      // init
+      if ((e = capture_into(G, tail))) return e;
+      HF_CUDA(cudaEventRecordWithFlags(bg->t0[i], cap, cudaEventRecordExternal));
+      k_cg_graph_begin<<<1, 1, 0, cap>>>(v.r.a);
+      HF_LAUNCH_CHECK("k_cg_graph_begin");
+      if ((e = v.init_ops(it.P0))) return e;
+      if ((e = end_capture(&tail))) return e;
+      // iteration loops
+      if (cf->max_iter > 0) {
+        const bool mixed = cf->fp32_exchange != 0;
+        for (int phase = mixed ? 0 : 1; phase < 2; ++phase) {
+          const bool f32 = phase == 0;
+          if (mixed && !f32) {  // the FP32 -> FP64 switch between the two loops
+            if ((e = capture_into(G, tail))) return e;
+            k_cg_graph_switch<<<1, 1, 0, cap>>>(v.r.a);
+            HF_LAUNCH_CHECK("k_cg_graph_switch");
+            if ((e = end_capture(&tail))) return e;
+          }
+          cudaGraphConditionalHandle h;
+          HF_CUDA(cudaGraphConditionalHandleCreate(&h, G, 1u, cudaGraphCondAssignDefault));
+          cudaGraphNodeParams np = {};
+          np.type = cudaGraphNodeTypeConditional;
+          np.conditional.handle = h;
+          np.conditional.type = cudaGraphCondTypeWhile;
+          np.conditional.size = 1;
+          cudaGraphNode_t loop = nullptr;
+          HF_CUDA(cudaGraphAddNode(&loop, G, tail.empty() ? nullptr : tail.data(), tail.size(), &np));
+          cudaGraph_t body = np.conditional.phGraph_out[0];
+          if ((e = capture_into(body, {}))) return e;
+          if ((e = cg_iteration(v.r, cap, *cf, f32))) return e;
+          k_cg_graph_cond<<<1, 1, 0, cap>>>(h, v.r.a, f32 ? cf->max_iter / 2 : cf->max_iter);
+          HF_LAUNCH_CHECK("k_cg_graph_cond");
+          if ((e = end_capture(nullptr))) return e;
+          tail.assign(1, loop);
+        }
+      }
+      // finalize
+      if ((e = capture_into(G, tail))) return e;
+      if ((e = v.finalize_ops(true))) return e;
+      HF_CUDA(cudaEventRecordWithFlags(bg->t1[i], cap, cudaEventRecordExternal));
+      if ((e = end_capture(nullptr))) return e;
+    }
+    HF_CUDA(cudaGraphInstantiate(&bg->exec, G, 0));
+    HF_CUDA(cudaStreamCreateWithFlags(&bg->run, cudaStreamNonBlocking));
+    HF_CUDA(cudaEventCreateWithFlags(&bg->ev_in, cudaEventDisableTiming));
+    HF_CUDA(cudaEventCreateWithFlags(&bg->ev_out, cudaEventDisableTiming));
+    return HF_OK;
+  };
+  st = build();
+  if (cap) {
+    if (st != HF_OK) {  // leave no capture open on an error path
+      cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+      if (cudaStreamIsCapturing(cap, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(cap, &g);
+      }
+      cudaGetLastError();
+    }
+    cudaStreamDestroy(cap);
+  }
+  if (st != HF_OK) {
+    delete bg;
+    return st;
+  }
+  *handle = bg;
+  return HF_OK;
+}
+
+// Runs a built batch after the work already queued on `stream` and makes `stream` wait
+// for it; with solve_ms (n_items entries) it waits for the batch and fills each solve's
+// device time from its start to its final scalars.
+extern "C" int hf_cg_batch_graph_launch(void* handle, void* stream, double* solve_ms) {
+  if (!handle) return fail(HF_ERR_INVALID, "NULL batch graph");
+  auto* bg = static_cast<CgBatchGraph*>(handle);
+  cudaStream_t user = static_cast<cudaStream_t>(stream);
+  HF_CUDA(cudaEventRecord(bg->ev_in, user));
+  HF_CUDA(cudaStreamWaitEvent(bg->run, bg->ev_in, 0));
+  HF_CUDA(cudaGraphLaunch(bg->exec, bg->run));
+  HF_CUDA(cudaEventRecord(bg->ev_out, bg->run));
+  HF_CUDA(cudaStreamWaitEvent(user, bg->ev_out, 0));
+  if (solve_ms) {
+    HF_CUDA(cudaStreamSynchronize(bg->run));
+    for (int i = 0; i < bg->n; ++i) {
+      float ms = 0.f;
+      HF_CUDA(cudaEventElapsedTime(&ms, bg->t0[i], bg->t1[i]));
+      solve_ms[i] = ms;
+    }
+  }
+  return HF_OK;
+}
+
+extern "C" int hf_cg_batch_graph_destroy(void* handle) {
+  delete static_cast<CgBatchGraph*>(handle);
+  return HF_OK;
+}
+
+extern "C" int hf_cg_solve_batch_graph(void* stream, const hf_cg_batch_item* items, int n_items,
+                                       const hf_cg_config* cf, void* workspace, size_t bytes_per_item,
+                                       double* solve_ms) {
+  void* h = nullptr;
+  int st = hf_cg_batch_graph_create(items, n_items, cf, workspace, bytes_per_item, &h);
+  if (st) return st;
+  st = hf_cg_batch_graph_launch(h, stream, solve_ms);
+  if (st == HF_OK && !solve_ms) {
+    const cudaError_t e = cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) st = cuda_check(e, "cudaStreamSynchronize");
+  }
+  hf_cg_batch_graph_destroy(h);
+  return st;
 }

@@ -339,7 +339,7 @@ class _CgBatchItem(C.Structure):
 
 
 def solve_batch(kernels, P0s, n_electrons, *, config: SolverConfig | None = None, lanes: int = 8,
-                return_times: bool = False, autotune: bool = False):
+                return_times: bool = False, autotune: bool = False, graph: bool = False):
     """Many independent CG solves in one native call (density scans).
 
     ``kernels``, ``P0s`` and ``n_electrons`` are equal-length sequences; each
@@ -351,6 +351,10 @@ def solve_batch(kernels, P0s, n_electrons, *, config: SolverConfig | None = None
     ``autotune=True`` first runs the Fock-schedule autotuner (``hf_fock_autotune``) once for
     every distinct (mesh, nb, Fock flags) of the scan, on that solve's P0; the stored choices
     then apply to every build of the batch.
+    ``graph=True`` runs the whole batch as one CUDA graph launched once
+    (``hf_cg_solve_batch_graph``): every solve a branch whose iteration loop is a
+    device-side conditional node, all solves at once with a workspace each (``lanes``
+    is then unused); the results are those of the stream driver.
     """
     cfg = config or SolverConfig()
     if str(cfg.optimizer).lower() != "cg":
@@ -362,23 +366,60 @@ def solve_batch(kernels, P0s, n_electrons, *, config: SolverConfig | None = None
         raise ValueError("kernels, P0s and n_electrons must be non-empty and of equal length.")
     L = _lib.lib()
     dev = kernels[0].device
+    if autotune:
+        _autotune_scan(kernels, P0s, cfg)
+    items, outs, keep, scs, conf, per_lane = _batch_items(kernels, P0s, n_electrons, cfg)
+    lanes = max(1, min(int(lanes), n))
+    times = (C.c_double * n)()
+    if graph:
+        ws = _lib.workspace(n * per_lane, dev, "cg_batch")
+        _lib.check(L.hf_cg_solve_batch_graph(_lib.stream_ptr(dev), items, n, C.byref(conf), ws.data_ptr(),
+                                             per_lane, times))
+    else:
+        ws = _lib.workspace(lanes * per_lane, dev, "cg_batch")
+        _lib.check(L.hf_cg_solve_batch(_lib.stream_ptr(dev), items, n, C.byref(conf), lanes, ws.data_ptr(),
+                                       per_lane, times))
+    results = _batch_results(outs, scs, cfg)
+    del keep
+    times = list(times)
+    if str(cfg.polish).lower() == "scf":
+        # the FP64 polish of every solve, on concurrent streams (one host thread each)
+        from .reference_scf import SCFConfig, solve_scf_batch
+        pol = solve_scf_batch(kernels, [r.density for r in results], list(n_electrons),
+                              config=SCFConfig(acceleration="diis", density_tol=float(cfg.polish_density_tol),
+                                               comm_tol=float(cfg.polish_comm_tol),
+                                               max_iter=int(cfg.polish_max_iter), mu_method="newton",
+                                               warm_eigh=True),
+                              workers=lanes, return_times=True)
+        results = [_from_scf(k, r, res.n_iter, res.history, float(res.energy))
+                   for k, r, res in zip(kernels, pol[0], results)]
+        times = [a + b for a, b in zip(times, pol[1])]
+    return (results, times) if return_times else results
+
+
+def _autotune_scan(kernels, P0s, cfg):
+    seen = set()
+    for kern, P0 in zip(kernels, P0s):
+        kc = KernelC128(kern)
+        for fp32 in ((False, True) if cfg.fp32_exchange else (False,)):
+            key = (tuple(kern.shape), kc.flags(), fp32)
+            if key not in seen:
+                seen.add(key)
+                kc.autotune(P0, fp32=fp32)
+
+
+def _batch_items(kernels, P0s, n_electrons, cfg):
+    """The C batch items of a scan: every output a view of one allocation (one allocator call per
+    batch instead of seven per solve; the block lives as long as any returned tensor does)."""
+    L = _lib.lib()
+    n = len(kernels)
+    dev = kernels[0].device
     conf = _CgConfig(int(cfg.max_iter), float(cfg.tol_E), float(cfg.tol_grad), float(cfg.denom_scale),
                      float(cfg.max_step), int(cfg.cg_restart), float(cfg.bt_shrink), int(cfg.bt_max),
                      int(cfg.mu_maxiter), int(cfg.plateau_window), int(bool(cfg.fp32_exchange)),
                      float(cfg.fp32_switch_rel), int(cfg.chunk), FOCK_CB(), PROJECT_CB(), None)
-    if autotune:
-        seen = set()
-        for kern, P0 in zip(kernels, P0s):
-            kc = KernelC128(kern)
-            for fp32 in ((False, True) if cfg.fp32_exchange else (False,)):
-                key = (tuple(kern.shape), kc.flags(), fp32)
-                if key not in seen:
-                    seen.add(key)
-                    kc.autotune(P0, fp32=fp32)
     items = (_CgBatchItem * n)()
     keep, outs = [], []
-    # All outputs of the batch are views of one allocation (one allocator call per batch instead of
-    # seven per solve); the block lives as long as any returned tensor does.
     nh = max(cfg.max_iter, 1)
     shapes = [tuple(k.shape) for k in kernels]
     al = lambda b: (b + 255) // 256 * 256
@@ -414,35 +455,77 @@ def solve_batch(kernels, P0s, n_electrons, *, config: SolverConfig | None = None
         outs.append((kern, Q, p, P, F, hE, hG, sc))
     per_lane = C.c_size_t(0)
     _lib.check(L.hf_cg_batch_workspace_size(items, n, C.byref(conf), C.byref(per_lane)))
-    lanes = max(1, min(int(lanes), n))
-    ws = _lib.workspace(lanes * per_lane.value, dev, "cg_batch")
-    times = (C.c_double * n)()
-    _lib.check(L.hf_cg_solve_batch(_lib.stream_ptr(dev), items, n, C.byref(conf), lanes, ws.data_ptr(),
-                                   per_lane.value, times))
+    return items, outs, keep, scs, conf, per_lane.value
+
+
+def _batch_results(outs, scs, cfg, copy=False):
     results = []
     host = scs.cpu().numpy()
+    cp = (lambda t: t.clone()) if copy else (lambda t: t)
     for i, (kern, Q, p, P, F, hE, hG, sc) in enumerate(outs):
         s = host[i]
-        hist = dict(E=hE[:cfg.max_iter].to(kern.real_dtype), grad_norm=hG[:cfg.max_iter].to(kern.real_dtype),
+        hist = dict(E=cp(hE[:cfg.max_iter].to(kern.real_dtype)), grad_norm=cp(hG[:cfg.max_iter].to(kern.real_dtype)),
                     fp32_switch_iter=int(s[5]))
-        results.append(SolveResult(Q=Q.to(kern.dtype), p=p.to(kern.real_dtype), mu=sc[0].to(kern.real_dtype),
-                                   density=P.to(kern.dtype), fock=F.to(kern.dtype), energy=sc[1].clone(),
+        results.append(SolveResult(Q=cp(Q.to(kern.dtype)), p=cp(p.to(kern.real_dtype)), mu=sc[0].to(kern.real_dtype).clone(),
+                                   density=cp(P.to(kern.dtype)), fock=cp(F.to(kern.dtype)), energy=sc[1].clone(),
                                    n_iter=torch.tensor(int(s[2]), dtype=torch.int32),
                                    converged=torch.tensor(bool(s[3])), history=hist))
-    del keep
-    times = list(times)
-    if str(cfg.polish).lower() == "scf":
-        # the FP64 polish of every solve, on concurrent streams (one host thread each)
-        import time as _time
-        from .reference_scf import SCFConfig, solve_scf_batch
-        t0 = _time.perf_counter()
-        pol = solve_scf_batch(kernels, [r.density for r in results], list(n_electrons),
-                              config=SCFConfig(acceleration="diis", density_tol=float(cfg.polish_density_tol),
-                                               comm_tol=float(cfg.polish_comm_tol),
-                                               max_iter=int(cfg.polish_max_iter), mu_method="newton",
-                                               warm_eigh=True),
-                              workers=lanes, return_times=True)
-        results = [_from_scf(k, r, res.n_iter, res.history, float(res.energy))
-                   for k, r, res in zip(kernels, pol[0], results)]
-        times = [a + b for a, b in zip(times, pol[1])]
-    return (results, times) if return_times else results
+    return results
+
+
+class ScanGraph:
+    """A batch of CG solves captured once as ONE CUDA graph (``hf_cg_batch_graph_create``) and
+    launched any number of times (no reference counterpart; the reference loops ``solve``).
+
+    Every solve is a branch of the graph whose iteration loop is a device-side conditional
+    node, so a launch runs the whole scan without a host round trip.  ``run(P0s=None)``
+    writes new starting densities (same shapes) into the graph's P0 buffers, launches and
+    returns fresh ``SolveResult``s (and each solve's device time with ``return_times``).
+    ``launch()`` only enqueues the graph on the current stream.  Hooks are not supported
+    (``optimizer="cg"`` without project_fn / block_sizes)."""
+
+    def __init__(self, kernels, P0s, n_electrons, *, config: SolverConfig | None = None, autotune: bool = False):
+        cfg = config or SolverConfig()
+        if str(cfg.optimizer).lower() != "cg" or cfg.project_fn is not None or cfg.block_sizes is not None:
+            raise ValueError("ScanGraph runs the CG optimizer without hooks.")
+        n = len(kernels)
+        if n == 0 or len(P0s) != n or len(n_electrons) != n:
+            raise ValueError("kernels, P0s and n_electrons must be non-empty and of equal length.")
+        if autotune:
+            _autotune_scan(kernels, P0s, cfg)
+        self.cfg = cfg
+        self.L = _lib.lib()
+        self.dev = kernels[0].device
+        self.items, self.outs, self.keep, self.scs, self.conf, per = _batch_items(kernels, P0s, n_electrons, cfg)
+        self.P0 = [k for k in self.keep if isinstance(k, torch.Tensor)]
+        self.ws = torch.empty(max(n * per, 256), dtype=torch.uint8, device=self.dev)
+        h = C.c_void_p(None)
+        _lib.check(self.L.hf_cg_batch_graph_create(self.items, n, C.byref(self.conf), self.ws.data_ptr(), per,
+                                                   C.byref(h)))
+        self.handle = h
+        self.n = n
+
+    def launch(self, times=None):
+        _lib.check(self.L.hf_cg_batch_graph_launch(self.handle, _lib.stream_ptr(self.dev), times))
+
+    def run(self, P0s=None, return_times: bool = False):
+        if P0s is not None:
+            if len(P0s) != self.n:
+                raise ValueError(f"expected {self.n} starting densities, got {len(P0s)}")
+            for dst, src in zip(self.P0, P0s):
+                dst.copy_(torch.as_tensor(src).to(self.dev, torch.complex128).reshape(dst.shape))
+        times = (C.c_double * self.n)()
+        self.launch(times)
+        res = _batch_results(self.outs, self.scs, self.cfg, copy=True)
+        return (res, list(times)) if return_times else res
+
+    def close(self):
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            self.L.hf_cg_batch_graph_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -154,6 +154,54 @@ def test_cg_batch_matches_single_solves(cuda, mixed):
         assert r.history["fp32_switch_iter"] == r1.history["fp32_switch_iter"]
 
 
+@pytest.mark.parametrize("mixed", [False, True])
+def test_cg_batch_graph_matches_stream_driver(cuda, mixed):
+    """hf_cg_solve_batch_graph (the whole batch as one CUDA graph with device-side loops):
+    every solve equals the stream driver's, iteration counts and switch points included."""
+    import jax_hf_b200 as G
+    from jax_hf_b200.solver import SolverConfig, solve_batch
+    probs = _scan_problems()
+    cfg = SolverConfig(max_iter=150, tol_E=1e-10, fp32_exchange=mixed)
+    Ks = [G.HartreeFockKernel(**p.kernel_kwargs()) for p in probs]
+    P0s = [np.zeros((p.nk, p.nk, p.nb, p.nb), complex) for p in probs]
+    nes = [p.n_electrons for p in probs]
+    ref = solve_batch(Ks, P0s, nes, config=cfg, lanes=2)
+    res, times = solve_batch(Ks, P0s, nes, config=cfg, graph=True, return_times=True)
+    assert len(res) == len(probs) and all(t > 0 for t in times)
+    for r, r1 in zip(res, ref):
+        assert int(r.n_iter) == int(r1.n_iter)
+        assert bool(r.converged) == bool(r1.converged)
+        assert float(r.energy) == float(r1.energy)
+        assert torch.equal(r.density, r1.density)
+        assert torch.equal(r.Q, r1.Q)
+        assert r.history["fp32_switch_iter"] == r1.history["fp32_switch_iter"]
+
+
+def test_scan_graph_relaunch_with_new_starting_densities(cuda):
+    """ScanGraph: captured once, launched twice with different P0s; each launch equals the
+    stream driver's batch on the same P0s, and the first launch's results are not overwritten."""
+    import jax_hf_b200 as G
+    from jax_hf_b200 import synthetic as S2
+    from jax_hf_b200.solver import ScanGraph, SolverConfig, solve_batch
+    probs = _scan_problems()[:4]
+    cfg = SolverConfig(max_iter=150, tol_E=1e-10)
+    Ks = [G.HartreeFockKernel(**p.kernel_kwargs()) for p in probs]
+    nes = [p.n_electrons for p in probs]
+    P0a = [np.zeros((p.nk, p.nk, p.nb, p.nb), complex) for p in probs]
+    P0b = [0.3 * S2.haar_density(p.nk, p.nb, 90 + i) for i, p in enumerate(probs)]
+    sg = ScanGraph(Ks, P0a, nes, config=cfg)
+    ra = sg.run()
+    rb, tb = sg.run(P0b, return_times=True)
+    sg.close()
+    assert all(t > 0 for t in tb)
+    for mine, P0s in ((ra, P0a), (rb, P0b)):
+        ref = solve_batch(Ks, P0s, nes, config=cfg, lanes=2)
+        for r, r1 in zip(mine, ref):
+            assert int(r.n_iter) == int(r1.n_iter)
+            assert float(r.energy) == float(r1.energy)
+            assert torch.equal(r.density, r1.density)
+
+
 def test_cg_batch_matches_oracle(cuda):
     """Batched FP64 solves against the oracle's CG on the same inputs."""
     import jax_hf_b200 as G
