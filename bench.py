@@ -360,6 +360,7 @@ def run_solves(dev):
     batched, the FP64 SCF-DIIS with the reference's steps solve by solve (the plain FP64
     path that reaches |dE/E| <= 1e-9), and the mixed solvers batched.
     """
+    import time as _time_mod
     import torch
     import jax_hf_b200 as G
     from jax_hf_b200 import synthetic as S
@@ -499,11 +500,23 @@ def run_solves(dev):
     legs = (("fp64_batched", "CG, tol_E 1e-9, 16 streams",
              lambda: solve_batch(Ks, P0s, nes, config=c64, lanes=16, return_times=True)),
             ("mixed_batched", "SCF-DIIS, FP32 exchange until density residual 1e-5 then FP64, Newton mu, warm eigh, "
-             "8 streams", lambda: solve_scf_batch(Ks, P0s, nes, config=mixed_scf, workers=8, return_times=True)),
-            ("fp64_fast_scf_batched", "SCF-DIIS, FP64 throughout, Newton mu, warm eigh, 8 streams",
-             lambda: solve_scf_batch(Ks, P0s, nes, config=fp64_fast, workers=8, return_times=True)),
+             "the whole batch as one CUDA graph (loops and DIIS solve on the device), captured once, launched per run",
+             lambda: mixed_graph.run(return_times=True)),
+            ("mixed_batched_host_threads", "the same mixed SCF-DIIS, 8 host threads with a stream each",
+             lambda: solve_scf_batch(Ks, P0s, nes, config=mixed_scf, workers=8, return_times=True)),
+            ("fp64_fast_scf_batched", "SCF-DIIS, FP64 throughout, Newton mu, warm eigh, one CUDA graph as above",
+             lambda: fp64_graph.run(return_times=True)),
             ("mixed_cg_polish_batched", "FP32-exchange CG to tol_E 1e-6, then FP64 SCF-DIIS polish, 16 streams",
              lambda: solve_batch(Ks, P0s, nes, config=mixed_cg, lanes=16, return_times=True)))
+    # the SCF batches as CUDA graphs (built once, outside the timed runs)
+    from jax_hf_b200.reference_scf import ScfScanGraph
+    t_b = _time_mod.perf_counter()
+    mixed_graph = ScfScanGraph(Ks, P0s, nes, config=mixed_scf)
+    scf_build_ms = (_time_mod.perf_counter() - t_b) * 1e3
+    fp64_graph = ScfScanGraph(Ks, P0s, nes, config=fp64_fast)
+    mixed_graph.run()
+    fp64_graph.run()
+    scan["scf_graph_build_ms_host_once"] = round(scf_build_ms, 1)
     # the FP64 CG batch as one CUDA graph (device-side loops), captured once and launched
     from jax_hf_b200.solver import ScanGraph
     import time as _time
@@ -532,6 +545,8 @@ def run_solves(dev):
                       "speedup_vs_fp64_scf_solve_by_solve": round(sum(t_scf) / ms, 3),
                       "speedup_vs_fp64_fast_scf_solve_by_solve": round(sum(t_fs) / ms, 3),
                       **errors([float(r.energy) for r in rb])}
+    mixed_graph.close()
+    fp64_graph.close()
     out["density_scan_64"] = scan
     out["gradients_96x96_nb4"] = run_gradients(dev, ev_time, base["newton_96x96_nb4"])
     import torch.distributed as dist

@@ -453,6 +453,40 @@ int hf_scf_solve(void* stream, const hf_cg_problem* problem, const hf_scf_config
                  void* density, void* fock, double* hist_E, double* hist_D, double* hist_C, double* scalars_out,
                  void* workspace, size_t workspace_bytes);
 
+/* A batch of independent SCF solves as ONE CUDA graph (extension, no reference
+ * counterpart): the loop of hf_scf_solve with its decisions on the device, so that no
+ * host round trip happens between the launch and the end of the last solve.  Every
+ * solve is a branch: init -> iteration 0 -> [WHILE FP32 iterations -> switch] ->
+ * WHILE FP64 iterations -> final FP64 build; the DIIS bordered system is solved by a
+ * one-thread kernel with the host driver's LU, and DIIS-or-mixing is a conditional IF
+ * node.  DIIS and linear mixing with every hf_scf_config option except ODA
+ * (acceleration 2) and the trust-radius clip (HF_ERR_UNSUPPORTED: they read values
+ * on the host every iteration).  Items: the problem, P0, the outputs (density, fock),
+ * per-iteration histories (DEVICE, max_iter float64 each, may be NULL) and scalars_out
+ * (DEVICE, 5 float64: energy, mu, iterations, converged, first FP64 iteration or -1).
+ * The workspace holds n_items blocks of bytes_per_item (hf_scf_batch_workspace_size).
+ * _create captures and instantiates (host work only), _launch runs the graph after
+ * the work queued on `stream` (solve_ms, may be NULL: waits and fills each solve's
+ * time), _destroy frees it; new starting densities may be written to the P0 buffers
+ * between launches. */
+typedef struct hf_scf_batch_item {
+  hf_cg_problem problem;
+  const void* P0;
+  void* density;
+  void* fock;
+  double* hist_E;
+  double* hist_D;
+  double* hist_C;
+  double* scalars_out;
+} hf_scf_batch_item;
+
+int hf_scf_batch_workspace_size(const hf_scf_batch_item* items, int n_items, const hf_scf_config* config,
+                                size_t* bytes_per_item);
+int hf_scf_batch_graph_create(const hf_scf_batch_item* items, int n_items, const hf_scf_config* config,
+                              void* workspace, size_t bytes_per_item, void** handle);
+int hf_scf_batch_graph_launch(void* handle, void* stream, double* solve_ms);
+int hf_scf_batch_graph_destroy(void* handle);
+
 /* ---- Trust-region Newton driver (complex128) -----------------------------------
  * Replaces jax_hf.solve with optimizer="newton" (solver.py:686-1078) for
  * project_fn=None, block_sizes=None and the built-in Fock build (nb <= 16):

@@ -98,6 +98,10 @@ _SIGS = {
     "hf_cg_batch_workspace_size": ([vp, i32, vp, psz], i32),
     "hf_scf_workspace_size": ([vp, vp, psz], i32),
     "hf_scf_solve": ([vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, sz], i32),
+    "hf_scf_batch_workspace_size": ([vp, i32, vp, psz], i32),
+    "hf_scf_batch_graph_create": ([vp, i32, vp, vp, sz, vp], i32),
+    "hf_scf_batch_graph_launch": ([vp, vp, vp], i32),
+    "hf_scf_batch_graph_destroy": ([vp], i32),
     "hf_newton_workspace_size": ([vp, vp, psz], i32),
     "hf_newton_solve": ([vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, sz], i32),
     "hf_fock_vjp_workspace_size": ([i32, u32, i32, i32, i32, psz], i32),

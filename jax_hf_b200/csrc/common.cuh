@@ -16,6 +16,13 @@ int fail(int status, const std::string& msg);
 int cuda_check(cudaError_t e, const char* what);
 int allow_max_dynamic_smem(const void* fn);
 int context_id(unsigned long long* id);
+// Slot-indexed DIIS steps for the device-resident SCF loop (ops.cu): the history slot is
+// a device int, so one captured iteration serves every slot
+int scf_residuals_slot(void* stream, int nk, int nb, const void* F, const void* P, const void* Pn, const double* w,
+                       void* R, size_t stride, const int* slot, void* delta, double* sums3, void* ws);
+int copy_to_slot(void* stream, size_t n, const void* x, void* hist, const int* slot);
+int gram_row_slot(void* stream, int n, const int* slot, size_t stride, int nk, int nb, const void* R,
+                  const double* w, double* b_out, void* ws);
 // P = herm(Q diag(p) Q^H), complex128, nb <= 8, lane-per-column kernel (solver_cg.cu)
 int rows_density(void* stream, int nk, int nb, const void* Q, const double* p, void* P);
 int symbol_address(const void* symbol, void** out);

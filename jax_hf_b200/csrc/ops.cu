@@ -69,9 +69,12 @@ __global__ void k_fermi(size_t n, const double* __restrict__ eps, const double* 
 
 // --------------------------------------------------------- SCF residuals --
 // delta = Pn - P, comm = F P - P F (stored), sums: w|delta|^2, w|comm|^2, w Re tr(F delta)
+// comm_slot (may be NULL): comm is the history slot *comm_slot of comm_stride elements each
 __global__ void k_scf_residuals(int nk, int nb, const double2* __restrict__ F, const double2* __restrict__ P,
                                 const double2* __restrict__ Pn, const double* __restrict__ w,
-                                double2* __restrict__ comm, double2* __restrict__ delta, double* part) {
+                                double2* __restrict__ comm, double2* __restrict__ delta, double* part,
+                                const int* __restrict__ comm_slot, size_t comm_stride) {
+  if (comm && comm_slot) comm += (size_t)(*comm_slot) * comm_stride;
   extern __shared__ double2 smd[];
   __shared__ double red[64];
   const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5, wpb = blockDim.x >> 5;
@@ -152,7 +155,8 @@ __global__ void k_gram(size_t stride, size_t len, int nb2, const double2* __rest
 // entry is formed exactly as in k_gram (fma(x_i, x_j, y_i y_j) is symmetric in i, j).
 template <int N>
 __global__ void k_gram_row(size_t stride, size_t len, int nb2, const double2* __restrict__ R, int inew,
-                           const double* __restrict__ w, double* part) {
+                           const double* __restrict__ w, double* part, const int* __restrict__ inew_dev = nullptr) {
+  if (inew_dev) inew = *inew_dev;
   __shared__ double red[64];
   double acc[N];
 #pragma unroll
@@ -464,8 +468,54 @@ extern "C" int hf_scf_residuals(void* stream, int nk, int nb, const void* F, con
   const size_t sm = (size_t)3 * nb * nb * sizeof(double2) * 4;
   HF_SMEM_CAP(k_scf_residuals);
   k_scf_residuals<<<g, 128, sm, HF_S>>>(nk, nb, (const double2*)F, (const double2*)P, (const double2*)Pn, w,
-                                        (double2*)comm, (double2*)delta, (double*)ws);
+                                        (double2*)comm, (double2*)delta, (double*)ws, nullptr, 0);
   return finish(HF_S, (double*)ws, g, 3, sums3);
+}
+
+// The SCF steps of a DIIS history whose current slot is a device int (the device-resident
+// SCF loop): residuals with the commutator into slot *slot of R, F copied into slot *slot
+// of Fhist, and row *slot of the Gram matrix.
+int hf::scf_residuals_slot(void* stream, int nk, int nb, const void* F, const void* P, const void* Pn,
+                           const double* w, void* R, size_t stride, const int* slot, void* delta, double* sums3,
+                           void* ws) {
+  const int g = perk_grid(nk);
+  const size_t sm = (size_t)3 * nb * nb * sizeof(double2) * 4;
+  HF_SMEM_CAP(k_scf_residuals);
+  k_scf_residuals<<<g, 128, sm, HF_S>>>(nk, nb, (const double2*)F, (const double2*)P, (const double2*)Pn, w,
+                                        (double2*)R, (double2*)delta, (double*)ws, slot, stride);
+  return finish(HF_S, (double*)ws, g, 3, sums3);
+}
+
+__global__ void k_copy_to_slot(size_t n, const double2* __restrict__ x, double2* __restrict__ hist,
+                               const int* __restrict__ slot) {
+  double2* dst = hist + (size_t)(*slot) * n;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+    dst[e] = x[e];
+}
+
+int hf::copy_to_slot(void* stream, size_t n, const void* x, void* hist, const int* slot) {
+  k_copy_to_slot<<<nblocks(n), kOpsThreads, 0, HF_S>>>(n, (const double2*)x, (double2*)hist, slot);
+  HF_LAUNCH_CHECK("k_copy_to_slot");
+  return HF_OK;
+}
+
+int hf::gram_row_slot(void* stream, int n, const int* slot, size_t stride, int nk, int nb, const void* R,
+                      const double* w, double* b_out, void* ws) {
+  if (n < 1 || n > 16) return fail(HF_ERR_INVALID, "gram_row_slot: 1 <= n <= 16");
+  const size_t len = (size_t)nk * nb * nb;
+  const int g = nblocks(len);
+  switch (n) {
+#define HF_GRAM_ROW(N)                                                                                      \
+  case N:                                                                                                   \
+    k_gram_row<N><<<g, kOpsThreads, 0, HF_S>>>(stride, len, nb * nb, (const double2*)R, 0, w, (double*)ws, \
+                                                slot);                                                      \
+    break;
+    HF_GRAM_ROW(1) HF_GRAM_ROW(2) HF_GRAM_ROW(3) HF_GRAM_ROW(4) HF_GRAM_ROW(5) HF_GRAM_ROW(6) HF_GRAM_ROW(7)
+    HF_GRAM_ROW(8) HF_GRAM_ROW(9) HF_GRAM_ROW(10) HF_GRAM_ROW(11) HF_GRAM_ROW(12) HF_GRAM_ROW(13)
+    HF_GRAM_ROW(14) HF_GRAM_ROW(15) HF_GRAM_ROW(16)
+#undef HF_GRAM_ROW
+  }
+  return finish(HF_S, (double*)ws, g, n, b_out);
 }
 
 extern "C" int hf_gram(void* stream, int n, size_t stride, int nk, int nb, const void* R, const double* w,

@@ -357,8 +357,124 @@ def _worker_streams(dev, n):
     return pool[:n]
 
 
+class _ScfBatchItem(C.Structure):
+    pass
+
+
+def _scf_batch_item_type():
+    from .solver import _CgProblem
+    if not getattr(_ScfBatchItem, "_fields_", None):
+        _ScfBatchItem._fields_ = [("problem", _CgProblem), ("P0", C.c_void_p), ("density", C.c_void_p),
+                                  ("fock", C.c_void_p), ("hist_E", C.c_void_p), ("hist_D", C.c_void_p),
+                                  ("hist_C", C.c_void_p), ("scalars_out", C.c_void_p)]
+    return _ScfBatchItem
+
+
+def _scf_config_struct(cfg):
+    acc = {"linear": 0, "diis": 1, "oda": 2}[cfg.acceleration]
+    return _ScfConfig(int(cfg.max_iter), float(cfg.density_tol), float(cfg.comm_tol), float(cfg.mixing),
+                      float(cfg.level_shift), acc, int(cfg.diis_size), int(cfg.diis_start), float(cfg.diis_damping),
+                      float(cfg.trust_radius), int(bool(cfg.fp32_exchange)), float(cfg.fp32_switch_density),
+                      2 if cfg.mu_method == "newton" else 0, int(bool(cfg.warm_eigh)))
+
+
+class ScfScanGraph:
+    """A batch of SCF solves captured once as ONE CUDA graph (``hf_scf_batch_graph_create``)
+    and launched any number of times (extension; no reference counterpart).
+
+    The loop of ``solve_scf`` runs with its decisions on the device: every solve is a
+    branch of the graph whose iterations are device-side conditional loops, and the
+    DIIS system is solved on the device, so a launch runs the whole batch without a
+    host round trip.  Each result equals the library's SCF driver's (``solve_scf``)
+    to the rounding of the DIIS solve.  ``run(P0s=None)`` writes new starting densities
+    (same shapes), launches and returns fresh ``SCFResult``s; ``launch()`` only enqueues.
+    ODA, the trust-radius clip and ``project_fn`` are not supported."""
+
+    def __init__(self, kernels, P0s, n_electrons, *, config: SCFConfig | None = None):
+        from .solver import KernelC128
+        cfg = config or SCFConfig()
+        n = len(kernels)
+        if n == 0 or len(P0s) != n or len(n_electrons) != n:
+            raise ValueError("kernels, P0s and n_electrons must be non-empty and of equal length.")
+        if cfg.project_fn is not None or cfg.acceleration == "oda" or cfg.trust_radius > 0.0:
+            raise ValueError("ScfScanGraph runs DIIS or linear mixing without project_fn or trust radius.")
+        if cfg.acceleration == "diis" and cfg.diis_size > 16:
+            raise ValueError("ScfScanGraph: diis_size <= 16")
+        Item = _scf_batch_item_type()
+        self.L = _lib.lib()
+        self.cfg = cfg
+        self.dev = kernels[0].device
+        self.sc = _scf_config_struct(cfg)
+        cd = torch.complex128
+        m = max(int(cfg.max_iter), 1)
+        self.items = (Item * n)()
+        self.keep, self.outs = [], []
+        for i, (kern, P0, ne) in enumerate(zip(kernels, P0s, n_electrons)):
+            validate_electron_count(kern.w2d, kern.h.shape[-1], ne, context="n_electrons")
+            kc = KernelC128(kern)
+            P0d = torch.as_tensor(P0).to(self.dev, cd).contiguous().clone()
+            dens, fock = torch.empty_like(P0d), torch.empty_like(P0d)
+            hist = torch.zeros((3, m), dtype=torch.float64, device=self.dev)
+            out = torch.full((5,), -1.0, dtype=torch.float64, device=self.dev)
+            self.items[i] = Item(kc.problem(ne), P0d.data_ptr(), dens.data_ptr(), fock.data_ptr(), hist[0].data_ptr(),
+                                 hist[1].data_ptr(), hist[2].data_ptr(), out.data_ptr())
+            self.keep += [kc, P0d]
+            self.outs.append((kern, P0d, dens, fock, hist, out))
+        per = C.c_size_t(0)
+        _lib.check(self.L.hf_scf_batch_workspace_size(self.items, n, C.byref(self.sc), C.byref(per)))
+        self.ws = torch.empty(max(n * per.value, 256), dtype=torch.uint8, device=self.dev)
+        h = C.c_void_p(None)
+        _lib.check(self.L.hf_scf_batch_graph_create(self.items, n, C.byref(self.sc), self.ws.data_ptr(), per.value,
+                                                    C.byref(h)))
+        self.handle = h
+        self.n = n
+
+    def launch(self, times=None):
+        _lib.check(self.L.hf_scf_batch_graph_launch(self.handle, _lib.stream_ptr(self.dev), times))
+
+    def run(self, P0s=None, return_times: bool = False):
+        if P0s is not None:
+            if len(P0s) != self.n:
+                raise ValueError(f"expected {self.n} starting densities, got {len(P0s)}")
+            for (_, dst, *_), src in zip(self.outs, P0s):
+                dst.copy_(torch.as_tensor(src).to(self.dev, torch.complex128).reshape(dst.shape))
+        times = (C.c_double * self.n)()
+        self.launch(times)
+        results = []
+        for kern, _, dens, fock, hist, out in self.outs:
+            o = out.cpu().numpy()
+            n_iter = int(o[2])
+            converged = bool(o[3] != 0.0)
+            h = hist[:, :n_iter].cpu().numpy()
+            if converged:
+                message = f"converged in {n_iter} iterations"
+            else:
+                dr = h[1, -1] if n_iter > 0 else float("nan")
+                cr = h[2, -1] if n_iter > 0 else float("nan")
+                message = f"stopped after {n_iter} iterations (density_res={dr:.3e}, comm_res={cr:.3e})"
+            results.append(SCFResult(
+                density_matrix=dens.to(kern.dtype).clone(), fock_matrix=fock.to(kern.dtype).clone(),
+                energy=torch.tensor(float(o[0]), dtype=torch.float64, device=self.dev),
+                chemical_potential=torch.tensor(float(o[1]), dtype=torch.float64, device=self.dev),
+                iterations=n_iter, converged=converged, message=message,
+                history={"E": h[0].copy(), "density_residual": h[1].copy(), "commutator_residual": h[2].copy(),
+                         "fp32_switch_iter": int(o[4]) if self.cfg.fp32_exchange else -1}))
+        return (results, list(times)) if return_times else results
+
+    def close(self):
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            self.L.hf_scf_batch_graph_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def solve_scf_batch(kernels, P0s, n_electrons, *, config: SCFConfig | None = None, workers: int = 16,
-                    return_times: bool = False):
+                    return_times: bool = False, graph: bool = False):
     """Many independent SCF solves at once (extension; density scans).
 
     Each solve has the semantics of ``solve_scf(kernel, P0, n, config=config)``
@@ -368,10 +484,18 @@ def solve_scf_batch(kernels, P0s, n_electrons, *, config: SCFConfig | None = Non
     thread, so the solves of the other streams keep the GPU busy.  Returns the
     list of ``SCFResult`` (and, with ``return_times``, each solve's wall time
     in ms, from its start on its stream to its final scalars).
+    ``graph=True`` runs the batch as one CUDA graph with the loops on the device
+    (``ScfScanGraph``, built and launched once; DIIS or linear mixing only).
     """
     import threading
     import time
     cfg = config or SCFConfig()
+    if graph:
+        sg = ScfScanGraph(kernels, P0s, n_electrons, config=cfg)
+        try:
+            return sg.run(return_times=return_times)
+        finally:
+            sg.close()
     n = len(kernels)
     if n == 0 or len(P0s) != n or len(n_electrons) != n:
         raise ValueError("kernels, P0s and n_electrons must be non-empty and of equal length.")

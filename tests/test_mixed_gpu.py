@@ -106,6 +106,46 @@ def test_scf_batch_equals_single_solves(cuda):
         assert float(a.energy) == float(b.energy)
 
 
+GRAPH_CFGS = [
+    ("mixed_fast", dict(FAST, fp32_exchange=True)),
+    ("fp64_fast", dict(FAST)),
+    ("reference_steps", dict(acceleration="diis", density_tol=1e-8, comm_tol=1e-7, max_iter=300)),
+    ("linear", dict(acceleration="linear", mixing=0.5, density_tol=1e-7, comm_tol=1e-6, max_iter=300)),
+    ("diis10_damped_shift", dict(acceleration="diis", diis_size=10, diis_damping=0.8, level_shift=0.2,
+                                 density_tol=1e-8, comm_tol=1e-7, max_iter=300)),
+]
+
+
+@pytest.mark.parametrize("name,cfg", GRAPH_CFGS, ids=[c[0] for c in GRAPH_CFGS])
+def test_scf_graph_batch_matches_single_solves(cuda, name, cfg):
+    """ScfScanGraph (the SCF loop on the device, the batch as one CUDA graph): every solve
+    takes the host driver's steps (iteration count, switch point, histories) and ends at its
+    energy and density."""
+    import jax_hf_b200 as G
+    from jax_hf_b200.reference_scf import SCFConfig, ScfScanGraph, solve_scf
+    probs = [(_fourier(12 + 4 * i, 4 + 2 * (i % 2), "layer" if i % 2 else "scalar", 0.1, 40 + i), 1.5 + 0.3 * i)
+             for i in range(4)]
+    Ks = [G.HartreeFockKernel(**kw) for kw, _ in probs]
+    P0s = [torch.zeros(np.asarray(kw["hamiltonian"]).shape, dtype=torch.complex128, device="cuda") for kw, _ in probs]
+    nes = [ne for _, ne in probs]
+    c = SCFConfig(**cfg)
+    sg = ScfScanGraph(Ks, P0s, nes, config=c)
+    res, times = sg.run(return_times=True)
+    res2 = sg.run()  # a second launch of the same graph
+    sg.close()
+    assert all(t > 0 for t in times)
+    for K, P0, ne, a, a2 in zip(Ks, P0s, nes, res, res2):
+        b = solve_scf(K, P0, ne, config=c)
+        assert a.iterations == b.iterations and a.converged == b.converged
+        assert a.history["fp32_switch_iter"] == b.history["fp32_switch_iter"]
+        np.testing.assert_allclose(a.history["E"], b.history["E"], rtol=1e-12, atol=1e-13)
+        np.testing.assert_allclose(a.history["density_residual"], b.history["density_residual"], rtol=1e-9,
+                                   atol=1e-15)
+        assert abs(float(a.energy) - float(b.energy)) <= 1e-12 * max(1.0, abs(float(b.energy)))
+        assert float((a.density_matrix - b.density_matrix).abs().max()) < 1e-10
+        assert float(a2.energy) == float(a.energy) and torch.equal(a2.density_matrix, a.density_matrix)
+
+
 @pytest.mark.parametrize("index", [3, 10, 17])
 def test_scan_fixture_problems(cuda, index):
     """Problems of the 64-solve density scan: the mixed SCF matches the committed oracle fixed
