@@ -635,9 +635,11 @@ __device__ __forceinline__ void jacobi_smem_cols(double2* SA, double2* SV, doubl
 // when Qin already diagonalises a nearby matrix, so the sweeps converge at once) and
 // Qout = Qin V.  Qin may equal Qout: a k-point's rows are read before they are written.
 constexpr int kEigWarps = 2;
+// mode 1 (no starting basis): the eigensolve of herm(i A), the Cayley spectral setup of
+// solver.py:161-166
 template <int NB>
 __device__ __forceinline__ void eig_cols(int nk, const double2* __restrict__ A, const double2* Qin, double2* Qout,
-                                         double* eps, double tol) {
+                                         double* eps, double tol, int mode = 0) {
   const bool rotate = Qin != nullptr;
   using RG = RowGroup<NB>;
   constexpr int G = RG::G, KPW = RG::KPW, LP = RG::LP, MAT = RG::MAT, NP = JacobiPairs<NB>::M / 2;
@@ -655,7 +657,10 @@ __device__ __forceinline__ void eig_cols(int nk, const double2* __restrict__ A, 
     const size_t base = (size_t)k * NB * NB + c;
     if (on) {
 #pragma unroll
-      for (int r = 0; r < NB; ++r) SA[r * LP + c] = A[base + (size_t)r * NB];
+      for (int r = 0; r < NB; ++r) {
+        const double2 x = A[base + (size_t)r * NB];
+        SA[r * LP + c] = mode ? make_double2(-x.y, x.x) : x;
+      }
     }
     if (rotate) {  // SA <- Q^H F Q, column c
       double2 q[NB], m[NB];
@@ -750,8 +755,8 @@ __global__ void __launch_bounds__(32 * kEigWarps, 8) k_cgr_eig(CgArgs a, const d
 template <int NB>
 __global__ void __launch_bounds__(32 * kEigWarps, 8) k_eig_cols(int nk, const double2* __restrict__ A,
                                                              const double2* Qin, double2* Qout, double* eps,
-                                                             double tol) {
-  eig_cols<NB>(nk, A, Qin, Qout, eps, tol);
+                                                             double tol, int mode) {
+  eig_cols<NB>(nk, A, Qin, Qout, eps, tol, mode);
 }
 
 }  // namespace hf

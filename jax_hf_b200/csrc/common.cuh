@@ -23,6 +23,9 @@ int scf_residuals_slot(void* stream, int nk, int nb, const void* F, const void* 
 int copy_to_slot(void* stream, size_t n, const void* x, void* hist, const int* slot);
 int gram_row_slot(void* stream, int n, const int* slot, size_t stride, int nk, int nb, const void* R,
                   const double* w, double* b_out, void* ws);
+// eigh of herm(A) (mode 0) or herm(i A) (mode 1), complex128, nb <= 8, ascending, the
+// lane-per-column Jacobi (solver_cg.cu)
+int eigh_cols(void* stream, int nk, int nb, const void* A, double* w, void* V, int mode);
 // P = herm(Q diag(p) Q^H), complex128, nb <= 8, lane-per-column kernel (solver_cg.cu)
 int rows_density(void* stream, int nk, int nb, const void* Q, const double* p, void* P);
 int symbol_address(const void* symbol, void** out);

@@ -283,6 +283,8 @@ static int eigh_common(void* stream, int dtype, int batch, int nb, int mode, con
   if (st) return st;
   if (batch == 0) return HF_OK;
   if (!A || !w || !V) return fail(HF_ERR_INVALID, "NULL argument");
+  // complex128 with nb <= 8: a group of lanes per matrix, one column per lane
+  if (dtype == HF_C128 && nb <= 8) return hf::eigh_cols(stream, batch, nb, A, static_cast<double*>(w), V, mode);
   Launch L = warp_launch(batch, jacobi_smem_elems(nb));
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (dtype == HF_C128) {

@@ -890,13 +890,28 @@ int rows_density(void* stream, int nk, int nb, const void* Q, const double* p, v
 
 template <int NB>
 static int eig_cols_launch(cudaStream_t s, int nk, const double2* A, const double2* Qin, double2* Qout,
-                           double* eps) {
+                           double* eps, int mode = 0) {
   const int per_block = kEigWarps * RowGroup<NB>::KPW;
   int b = (nk + per_block - 1) / per_block;
   if (b > 148 * 32) b = 148 * 32;
-  k_eig_cols<NB><<<b < 1 ? 1 : b, 32 * kEigWarps, 0, s>>>(nk, A, Qin, Qout, eps, kEigTol);
+  k_eig_cols<NB><<<b < 1 ? 1 : b, 32 * kEigWarps, 0, s>>>(nk, A, Qin, Qout, eps, kEigTol, mode);
   HF_LAUNCH_CHECK("k_eig_cols");
   return HF_OK;
+}
+
+// hf_eigh / hf_cayley_spectral for complex128 with nb <= 8 (perk.cu): the lane-per-column
+// Jacobi from the identity; mode 1 decomposes herm(i A)
+int eigh_cols(void* stream, int nk, int nb, const void* A, double* w, void* V, int mode) {
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  auto a = static_cast<const double2*>(A);
+  auto v = static_cast<double2*>(V);
+  switch (nb) {
+#define HF_NB_CASE(N) case N: return eig_cols_launch<N>(s, nk, a, nullptr, v, w, mode);
+    HF_NB_CASE(1) HF_NB_CASE(2) HF_NB_CASE(3) HF_NB_CASE(4) HF_NB_CASE(5) HF_NB_CASE(6) HF_NB_CASE(7) HF_NB_CASE(8)
+#undef HF_NB_CASE
+    default: break;
+  }
+  return fail(HF_ERR_UNSUPPORTED, "eigh_cols: nb > 8");
 }
 
 static int cg_iteration_warp(CgRun& r, cudaStream_t s, const hf_cg_config& cf, bool fp32);
