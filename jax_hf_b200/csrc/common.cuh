@@ -21,6 +21,10 @@ int context_id(unsigned long long* id);
 int scf_residuals_slot(void* stream, int nk, int nb, const void* F, const void* P, const void* Pn, const double* w,
                        void* R, size_t stride, const int* slot, void* delta, double* sums3, void* ws);
 int copy_to_slot(void* stream, size_t n, const void* x, void* hist, const int* slot);
+// n <= 4 inner products of hf_jdot's form in one pass, each equal to hf_jdot's (ops.cu)
+int jdot_multi(void* stream, size_t nk, int nb, int n, const void* const* aX, const void* const* bX,
+               const double* const* wX, const double* const* ap, const double* const* bp, const double* const* wp,
+               double* out, void* ws);
 int gram_row_slot(void* stream, int n, const int* slot, size_t stride, int nk, int nb, const void* R,
                   const double* w, double* b_out, void* ws);
 // eigh of herm(A) (mode 0) or herm(i A) (mode 1), complex128, nb <= 8, ascending, the

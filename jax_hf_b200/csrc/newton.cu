@@ -98,6 +98,13 @@ struct Newton {
   int jip(const void* aX, const double* ap, const void* bX, const double* bp, double* out) {
     return hf_jdot(s, (size_t)nk, nb, aX, bX, nullptr, ap, bp, w2d(), out, ops());
   }
+  // n of them in one pass, each equal to jip's
+  int jip_multi(int n, const void* const* aX, const double* const* ap, const void* const* bX,
+                const double* const* bp, double* out) {
+    const double* wx[4] = {nullptr, nullptr, nullptr, nullptr};
+    const double* wp[4] = {w2d(), w2d(), w2d(), w2d()};
+    return jdot_multi(s, (size_t)nk, nb, n, aX, bX, wx, ap, bp, wp, out, ops());
+  }
   // solver._solve_mu (solver.py:62-101) from the device seed mu0
   int solve_mu(const double* eps, const double* mu0, double* mu_out) {
     return hf_find_mu(s, HF_C128, 2, nk, 1, nb, eps, at<double>(oWN), n_target_norm, T_r, cf->mu_maxiter, mu0,
@@ -332,10 +339,13 @@ extern "C" int hf_newton_solve(void* stream, const hf_cg_problem* pb, const hf_n
     bool done = false;
     while (cg < cf->tr_cg_max && !done) {
       if ((st = N.hvp(Q, Ft, p, dX, dp, pen, HdX, Hdp))) return st;
-      if ((st = N.jip(dX, dp, HdX, Hdp, dots + 0))) return st;
-      if ((st = N.jip(dX, dp, dX, dp, dots + 1))) return st;
-      if ((st = N.jip(VX(vi), VP(vi), dX, dp, dots + 2))) return st;
-      if ((st = N.jip(VX(vi), VP(vi), VX(vi), VP(vi), dots + 3))) return st;
+      {  // d.Hd, d.d, v.d, v.v in one pass
+        const void* ax[4] = {dX, dX, VX(vi), VX(vi)};
+        const void* bx[4] = {HdX, dX, dX, VX(vi)};
+        const double* apv[4] = {dp, dp, VP(vi), VP(vi)};
+        const double* bpv[4] = {Hdp, dp, dp, VP(vi)};
+        if ((st = N.jip_multi(4, ax, apv, bx, bpv, dots + 0))) return st;
+      }
       double d4[4];
       if ((st = N.read(d4, dots, 4))) return st;
       const double dHd = d4[0], dd = d4[1];
@@ -348,12 +358,16 @@ extern "C" int hf_newton_solve(void* stream, const hf_cg_problem* pb, const hf_n
       const int va = 1 - vi, ra = 1 - ri;
       if ((st = hf_axpby(s, (size_t)nk, nb, 1.0, VX(vi), alpha, dX, 0, VX(va)))) return st;
       if ((st = hf_axpby_real(s, nv, 1.0, VP(vi), alpha, dp, VP(va)))) return st;
-      if ((st = N.jip(VX(va), VP(va), VX(va), VP(va), dots + 4))) return st;
       if ((st = hf_axpby(s, (size_t)nk, nb, 1.0, RX(ri), -alpha, HdX, 0, RX(ra)))) return st;
       if ((st = hf_axpby_real(s, nv, 1.0, RP(ri), -alpha, Hdp, RP(ra)))) return st;
-      if ((st = N.jip(RX(ra), RP(ra), RX(ra), RP(ra), dots + 5))) return st;
       if ((st = N.prec(RX(ra), RP(ra), eps, p, lam_pc, zX, zp))) return st;
-      if ((st = N.jip(RX(ra), RP(ra), zX, zp, dots + 6))) return st;
+      {  // |v + a d|^2, |r - a Hd|^2, r.z in one pass
+        const void* ax[3] = {VX(va), RX(ra), RX(ra)};
+        const void* bx[3] = {VX(va), RX(ra), zX};
+        const double* apv[3] = {VP(va), RP(ra), RP(ra)};
+        const double* bpv[3] = {VP(va), RP(ra), zp};
+        if ((st = N.jip_multi(3, ax, apv, bx, bpv, dots + 4))) return st;
+      }
       double d3[3];
       if ((st = N.read(d3, dots + 4, 3))) return st;
       const bool cross = std::sqrt(std::fmax(0.0, d3[0])) >= Delta;
@@ -386,9 +400,15 @@ extern "C" int hf_newton_solve(void* stream, const hf_cg_problem* pb, const hf_n
     // ---- predicted reduction and trial step (solver.py:998-1046) ----
     void* vX = VX(vi);
     double* vp = VP(vi);
-    if ((st = hf_jdot(s, (size_t)nk, nb, G, vX, w2d, nullptr, nullptr, nullptr, dots + 0, N.ops()))) return st;
-    if ((st = hf_jdot(s, (size_t)nk, nb, vX, HvX, w2d, vp, Hvp, w2d, dots + 1, N.ops()))) return st;
-    if ((st = N.jip(vX, vp, vX, vp, dots + 2))) return st;
+    {  // g.v, v.Hv, v.v in one pass
+      const void* ax[3] = {G, vX, vX};
+      const void* bx[3] = {vX, HvX, vX};
+      const double* wxv[3] = {w2d, w2d, nullptr};
+      const double* apv[3] = {nullptr, vp, vp};
+      const double* bpv[3] = {nullptr, Hvp, vp};
+      const double* wpv[3] = {nullptr, w2d, w2d};
+      if ((st = jdot_multi(s, (size_t)nk, nb, 3, ax, bx, wxv, apv, bpv, wpv, dots + 0, N.ops()))) return st;
+    }
     double m3[3];
     if ((st = N.read(m3, dots, 3))) return st;
     const double pred = -(m3[0] + 0.5 * m3[1]);

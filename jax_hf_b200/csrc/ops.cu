@@ -238,6 +238,52 @@ __global__ void k_jdot(size_t nk, int nb, const double2* __restrict__ aX, const 
   write_partials<1>(acc, part, red);
 }
 
+// Up to four joint inner products in one pass: product q is accumulated by every thread
+// exactly as k_jdot accumulates it (same grid, same elements, same order) and finished
+// with the same reductions, so each value equals the separate hf_jdot's bit for bit.
+struct JdotSpec {
+  const double2 *aX, *bX;
+  const double *wX, *ap, *bp, *wp;
+};
+struct JdotMulti {
+  JdotSpec d[4];
+  int n;
+};
+
+__global__ void k_jdot_multi(size_t nk, int nb, const __grid_constant__ JdotMulti m, double* part) {
+  __shared__ double red[64];
+  KSum acc[4];
+  const int nb2 = nb * nb;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    if (q >= m.n) break;
+    const JdotSpec& d = m.d[q];
+    if (d.aX) {
+      const size_t n = nk * nb2;
+      for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const double wk = d.wX ? d.wX[e / nb2] : 1.0;
+        acc[q].add(wk * (d.aX[e].x * d.bX[e].x + d.aX[e].y * d.bX[e].y));
+      }
+    }
+    if (d.ap) {
+      const size_t n = nk * nb;
+      for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const double wk = d.wp ? d.wp[e / nb] : 1.0;
+        acc[q].add(wk * d.ap[e] * d.bp[e]);
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    if (q >= m.n) break;
+    KSum r = block_reduce(acc[q], red);
+    if (threadIdx.x == 0) {
+      part[((size_t)blockIdx.x * m.n + q) * 2] = r.s;
+      part[((size_t)blockIdx.x * m.n + q) * 2 + 1] = r.c;
+    }
+  }
+}
+
 // ---------------------------------------------------------------- Newton --
 // G = skew((p_j - p_i) Ft) offdiag, eps = Re diag(Ft)                 (solver.py:898-900)
 __global__ void k_orbital_grad(size_t nk, int nb, const double2* __restrict__ Ft, const double* __restrict__ p,
@@ -582,6 +628,27 @@ extern "C" int hf_jdot(void* stream, size_t nk, int nb, const void* aX, const vo
   const int g = nblocks(nk * nb * nb);
   k_jdot<<<g, kOpsThreads, 0, HF_S>>>(nk, nb, (const double2*)aX, (const double2*)bX, wX, ap, bp, wp, (double*)ws);
   return finish(HF_S, (double*)ws, g, 1, out);
+}
+
+// n (1..4) joint inner products of hf_jdot's form into out[0..n) in one pass
+int hf::jdot_multi(void* stream, size_t nk, int nb, int n, const void* const* aX, const void* const* bX,
+                   const double* const* wX, const double* const* ap, const double* const* bp,
+                   const double* const* wp, double* out, void* ws) {
+  if (n < 1 || n > 4 || !out || !ws) return fail(HF_ERR_INVALID, "jdot_multi: 1 <= n <= 4");
+  JdotMulti m;
+  m.n = n;
+  for (int q = 0; q < 4; ++q) {
+    const bool on = q < n;
+    m.d[q].aX = on ? static_cast<const double2*>(aX[q]) : nullptr;
+    m.d[q].bX = on ? static_cast<const double2*>(bX[q]) : nullptr;
+    m.d[q].wX = on ? wX[q] : nullptr;
+    m.d[q].ap = on ? ap[q] : nullptr;
+    m.d[q].bp = on ? bp[q] : nullptr;
+    m.d[q].wp = on ? wp[q] : nullptr;
+  }
+  const int g = nblocks(nk * nb * nb);
+  k_jdot_multi<<<g, kOpsThreads, 0, HF_S>>>(nk, nb, m, (double*)ws);
+  return finish(HF_S, (double*)ws, g, n, out);
 }
 
 extern "C" int hf_orbital_grad(void* stream, size_t nk, int nb, const void* Ft, const double* p, void* G, double* eps) {
