@@ -435,7 +435,17 @@ int hf_cg_solve(void* stream, const hf_cg_problem* problem, const hf_cg_config* 
  *    (the same root to rounding; level_shift must be 0).
  *  - warm_eigh != 0 (nb <= 8): the eigendecompositions of the iterations after
  *    the first start from the previous iteration's eigenvectors (hf_eigh_warm);
- *    the same decomposition to the Jacobi tolerance, in fewer sweeps. */
+ *    the same decomposition to the Jacobi tolerance, in fewer sweeps.
+ * Hooks (solve_scf's fock_build_fn and project_fn, reference_scf.py:124-365): with
+ * fock_cb the driver calls fock_cb(cb_user, stream, P, Sigma, H, F) for every build
+ * instead of hf_fock_build (H: nb x nb; fp32_exchange is then refused); with
+ * project_cb it calls project_cb(cb_user, stream, X) where the reference applies
+ * herm(project(.)) instead of herm(.): X holds the unprojected array and the
+ * callback replaces it in place by herm(project(X)) (the density before each build,
+ * the built F, the new density, the DIIS density and the mixed density).  The
+ * pointers are the driver's buffers inside the caller's workspace or outputs; a
+ * callback enqueues its work on `stream` and returns 0, or nonzero to abort
+ * (HF_ERR_ABORTED). */
 typedef struct hf_scf_config {
   int max_iter;
   double density_tol, comm_tol, mixing, level_shift;
@@ -446,6 +456,9 @@ typedef struct hf_scf_config {
   double fp32_switch_density; /* extension */
   int mu_method;              /* extension: 0 bisection (reference), 2 Newton-bracket warm start */
   int warm_eigh;              /* extension: eigh from the previous iteration's eigenvectors (nb <= 8) */
+  hf_fock_callback fock_cb;       /* NULL: built-in hf_fock_build */
+  hf_project_callback project_cb; /* NULL: no projection           */
+  void* cb_user;
 } hf_scf_config;
 
 int hf_scf_workspace_size(const hf_cg_problem* problem, const hf_scf_config* config, size_t* bytes);

@@ -118,11 +118,32 @@ struct Scf {
   bool mu_warm = false;  // mu from the Newton-bracket solver started at the previous mu
   bool eig_warm = false; // eigh started from the eigenvectors in kV (the previous decomposition)
   bool eig_cols = false; // eigh by the lane-per-column Jacobi (warm_eigh mode, nb <= 8)
+  // herm(project(X)) in place (the caller's projector), or nothing without one
+  int project(void* X) {
+    if (!cf->project_cb) return HF_OK;
+    if (cf->project_cb(cf->cb_user, s, X) != 0) return fail(HF_ERR_ABORTED, "hf_scf_solve: project callback failed");
+    return HF_OK;
+  }
+  // out = herm(project(a x + b y)) (reference_scf.py:275-276 with a projector)
+  int herm_proj_axpby(double a, const void* x, double b, const void* y, void* out) {
+    if (!cf->project_cb) return herm_axpby(a, x, b, y, out);
+    int st;
+    if ((st = hf_axpby(s, (size_t)nk, nb, a, x, b, y, 0, out))) return st;
+    return project(out);
+  }
   int fock(const void* P, void* Sg, void* H, void* F) {
-    const unsigned flags = pb->fock_flags | (fp32 ? HF_FOCK_FFT_FP32 : 0u);
-    return hf_fock_build(s, HF_C128, flags, pb->nk1, pb->nk2, nb, P, pb->h, pb->VR, pb->refP, pb->HH,
-                         pb->w2d, pb->n_contact, pb->contact_g, pb->contact_Oi, pb->contact_Oj, Sg, H, F,
-                         at<void>(kFOCKWS), fock_ws);
+    int st;
+    if (cf->fock_cb) {
+      if (cf->fock_cb(cf->cb_user, s, P, Sg, H, F) != 0)
+        return fail(HF_ERR_ABORTED, "hf_scf_solve: Fock callback failed");
+    } else {
+      const unsigned flags = pb->fock_flags | (fp32 ? HF_FOCK_FFT_FP32 : 0u);
+      if ((st = hf_fock_build(s, HF_C128, flags, pb->nk1, pb->nk2, nb, P, pb->h, pb->VR, pb->refP, pb->HH,
+                              pb->w2d, pb->n_contact, pb->contact_g, pb->contact_Oi, pb->contact_Oj, Sg, H, F,
+                              at<void>(kFOCKWS), fock_ws)))
+        return st;
+    }
+    return project(F);  // build_fock(project_fn=...) returns herm(project(F))
   }
   int energy(const void* P, const void* Sg, const void* H, double* E) {
     // H from hf_fock_build is one nb x nb matrix for all k (H_mode 1); zero without Hartree
@@ -163,10 +184,11 @@ struct Scf {
   // reference_scf.py:78-84: herm(density) -> build -> energy -> next density
   int build_and_occupy(const void* dens, void* F, void* Pn) {
     int st;
-    if ((st = herm_axpby(1.0, dens, 0.0, nullptr, at<void>(kDH)))) return st;
+    if ((st = herm_proj_axpby(1.0, dens, 0.0, nullptr, at<void>(kDH)))) return st;
     if ((st = fock(at<void>(kDH), at<void>(kSG), at<void>(kH), F))) return st;
     if ((st = energy(at<void>(kDH), at<void>(kSG), at<void>(kH), scal() + kSE))) return st;
-    return density_from_fock(F, Pn);
+    if ((st = density_from_fock(F, Pn))) return st;
+    return project(Pn);
   }
   int read(double* host, const double* dev, int n) {
     HF_CUDA(cudaMemcpyAsync(host, dev, n * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -194,6 +216,8 @@ static int scf_check(const hf_cg_problem* pb, const hf_scf_config* cf) {
     return fail(HF_ERR_INVALID, "hf_scf: mu_method 2 needs level_shift = 0");
   if (cf->fp32_exchange && !(pb->fock_flags & HF_FOCK_EXCHANGE))
     return fail(HF_ERR_INVALID, "hf_scf: fp32_exchange needs the exchange term");
+  if (cf->fp32_exchange && cf->fock_cb)
+    return fail(HF_ERR_INVALID, "hf_scf: fp32_exchange applies to the built-in Fock build only");
   return HF_OK;
 }
 
@@ -325,8 +349,9 @@ extern "C" int hf_scf_solve(void* stream, const hf_cg_problem* pb, const hf_scf_
         }
         if ((st = S.herm_axpby(1.0, Fx, 0.0, nullptr, S.at<void>(kFH)))) return st;
         if ((st = S.density_from_fock(S.at<void>(kFH), updated))) return st;
+        if ((st = S.project(updated))) return st;
       } else {
-        if ((st = S.herm_axpby(1.0, density, cf->mixing, S.at<void>(kDELTA), updated))) return st;
+        if ((st = S.herm_proj_axpby(1.0, density, cf->mixing, S.at<void>(kDELTA), updated))) return st;
       }
     } else if (oda) {
       if ((st = S.fock(Pn, S.at<void>(kSG), S.at<void>(kH), S.at<void>(kFX)))) return st;
@@ -338,9 +363,9 @@ extern "C" int hf_scf_solve(void* stream, const hf_cg_problem* pb, const hf_scf_
       double lam;
       if (c2 > 1e-12) lam = std::fmin(std::fmax(-c1 / (2.0 * c2), 0.0), 1.0);
       else lam = c1 < 0.0 ? 1.0 : 0.0;
-      if ((st = S.herm_axpby(1.0, density, lam, S.at<void>(kDELTA), updated))) return st;
+      if ((st = S.herm_proj_axpby(1.0, density, lam, S.at<void>(kDELTA), updated))) return st;
     } else {
-      if ((st = S.herm_axpby(1.0, density, cf->mixing, S.at<void>(kDELTA), updated))) return st;
+      if ((st = S.herm_proj_axpby(1.0, density, cf->mixing, S.at<void>(kDELTA), updated))) return st;
     }
     if (cf->trust_radius > 0.0) {  // reference_scf.py:333-339
       if ((st = hf_axpby(s, (size_t)nk, nb, 1.0, updated, -1.0, density, 0, S.at<void>(kSTEP)))) return st;
@@ -352,7 +377,7 @@ extern "C" int hf_scf_solve(void* stream, const hf_cg_problem* pb, const hf_scf_
       const double sn = std::sqrt(red / wsum);
       if (sn > cf->trust_radius) {
         const double scale = cf->trust_radius / std::fmax(sn, 1e-30);
-        if ((st = S.herm_axpby(1.0, density, scale, S.at<void>(kSTEP), updated))) return st;
+        if ((st = S.herm_proj_axpby(1.0, density, scale, S.at<void>(kSTEP), updated))) return st;
       }
     }
     HF_CUDA(cudaMemcpyAsync(density, converged ? Pn : updated, qbytes, cudaMemcpyDeviceToDevice, s));
@@ -655,6 +680,7 @@ struct ScfBatchGraph {
 }  // namespace hf
 
 static int scf_graph_check(const hf_scf_config* cf) {
+  if (cf->fock_cb || cf->project_cb) return fail(HF_ERR_INVALID, "hf_scf_batch_graph: no host callbacks");
   if (cf->acceleration == 2) return fail(HF_ERR_UNSUPPORTED, "hf_scf_batch_graph: ODA reads values per iteration");
   if (cf->trust_radius > 0.0)
     return fail(HF_ERR_UNSUPPORTED, "hf_scf_batch_graph: the trust-radius clip reads values per iteration");

@@ -8,10 +8,11 @@ loop's scalar decisions are taken on the host from a few float64 reductions per
 iteration, as the reference does in its traced loop.  The (N+1)^2 bordered DIIS
 system is solved on the host with LAPACK (numpy), like jnp.linalg.solve on CPU.
 
-Without a project_fn or a custom fock_build_fn, solve_scf runs the same loop in
-the library's C++ driver (hf_scf_solve), which issues the same device operations
-and reads the loop's scalars once per iteration; the Python loop below serves the
-hooks (and USE_NATIVE = False).
+solve_scf runs the same loop in the library's C++ driver (hf_scf_solve), which
+issues the same device operations and reads the loop's scalars once per
+iteration; a project_fn or a custom fock_build_fn runs there as a host callback
+on the same stream.  The Python loop below is the same loop step for step
+(USE_NATIVE = False, or a DIIS history longer than 16).
 """
 
 from __future__ import annotations
@@ -29,8 +30,8 @@ from .linalg import eigh, density_from_Qp
 from .utils import validate_electron_count
 
 
-# solve_scf runs the library's SCF driver (hf_scf_solve) when no project_fn or custom
-# fock_build_fn is given; False keeps every call on the Python loop below.
+# solve_scf runs the library's SCF driver (hf_scf_solve; hooks as host callbacks);
+# False keeps every call on the Python loop below.
 USE_NATIVE = True
 
 
@@ -132,11 +133,11 @@ def solve_scf(kernel, P0, n_electrons: float, *, config: SCFConfig | None = None
     ops = _Ops(dev, nk1, nk2, nb)
     project = cfg.project_fn
     validate_electron_count(w2d, nb, n_electrons, context="n_electrons")
-    if USE_NATIVE and fock_build_fn is None and project is None and (cfg.acceleration != "diis" or cfg.diis_size <= 16):
-        return _solve_scf_native(kernel, P0, n_electrons, cfg)
+    if USE_NATIVE and (cfg.acceleration != "diis" or cfg.diis_size <= 16):
+        return _solve_scf_native(kernel, P0, n_electrons, cfg, fock_build_fn)
     if cfg.fp32_exchange or cfg.mu_method != "bisection" or cfg.warm_eigh:
-        raise ValueError("SCFConfig.fp32_exchange, mu_method='newton' and warm_eigh run in the library's SCF driver, "
-                         "which takes no project_fn or fock_build_fn.")
+        raise ValueError("SCFConfig.fp32_exchange, mu_method='newton' and warm_eigh run in the library's SCF driver "
+                         "(diis_size <= 16).")
     a = kernel.as_args()
     VR = a["VR"] if kernel.dtype == cd else (a["VR"].to(cd) if a["VR"].is_complex() else a["VR"].to(torch.float64))
     fock_kw = dict(h=h, VR=VR, refP=kernel.refP if kernel.dtype == cd else kernel.refP.to(cd), HH=kernel.HH.double(),
@@ -284,17 +285,42 @@ def solve_scf(kernel, P0, n_electrons: float, *, config: SCFConfig | None = None
 
 
 class _ScfConfig(C.Structure):
-    _fields_ = [("max_iter", C.c_int), ("density_tol", C.c_double), ("comm_tol", C.c_double),
-                ("mixing", C.c_double), ("level_shift", C.c_double), ("acceleration", C.c_int),
-                ("diis_size", C.c_int), ("diis_start", C.c_int), ("diis_damping", C.c_double),
-                ("trust_radius", C.c_double), ("fp32_exchange", C.c_int), ("fp32_switch_density", C.c_double),
-                ("mu_method", C.c_int), ("warm_eigh", C.c_int)]
+    pass
 
 
-def _solve_scf_native(kernel, P0, n_electrons, cfg):
+def _scf_config_type():
+    from .solver import FOCK_CB, PROJECT_CB
+    if not getattr(_ScfConfig, "_fields_", None):
+        _ScfConfig._fields_ = [("max_iter", C.c_int), ("density_tol", C.c_double), ("comm_tol", C.c_double),
+                               ("mixing", C.c_double), ("level_shift", C.c_double), ("acceleration", C.c_int),
+                               ("diis_size", C.c_int), ("diis_start", C.c_int), ("diis_damping", C.c_double),
+                               ("trust_radius", C.c_double), ("fp32_exchange", C.c_int),
+                               ("fp32_switch_density", C.c_double), ("mu_method", C.c_int), ("warm_eigh", C.c_int),
+                               ("fock_cb", FOCK_CB), ("project_cb", PROJECT_CB), ("cb_user", C.c_void_p)]
+    return _ScfConfig
+
+
+def _buffer_views(*tensors):
+    """Maps a device pointer inside one of ``tensors`` to a tensor view of the given shape (the
+    driver hands its callbacks pointers into the workspace and the output buffers)."""
+    bases = [(t.data_ptr(), t.numel() * t.element_size(), t.view(-1).view(torch.uint8)) for t in tensors]
+
+    def view(ptr, shape):
+        nbytes = int(np.prod(shape)) * 16
+        for b, n, flat in bases:
+            if b <= ptr and ptr + nbytes <= b + n:
+                return flat[ptr - b:ptr - b + nbytes].view(torch.complex128).view(shape)
+        raise RuntimeError("callback buffer outside the driver's allocations")
+
+    return view
+
+
+def _solve_scf_native(kernel, P0, n_electrons, cfg, fock_build_fn=None):
     """solve_scf through the library's SCF driver (hf_scf_solve): the same steps as the
-    loop above, sequenced in C++ with one small device->host read per iteration."""
-    from .solver import KernelC128, _CgProblem
+    loop above, sequenced in C++ with one small device->host read per iteration.  A
+    project_fn or a custom fock_build_fn runs as a host callback of the driver on the
+    same stream."""
+    from .solver import FOCK_CB, PROJECT_CB, KernelC128, _CgProblem
 
     L = _lib.lib()
     if not getattr(L, "_scf_bound", False):
@@ -309,24 +335,57 @@ def _solve_scf_native(kernel, P0, n_electrons, cfg):
     cd = torch.complex128
     kc = KernelC128(kernel)
     pb = kc.problem(n_electrons)
-    acc = {"linear": 0, "diis": 1, "oda": 2}[cfg.acceleration]
-    sc = _ScfConfig(int(cfg.max_iter), float(cfg.density_tol), float(cfg.comm_tol), float(cfg.mixing),
-                    float(cfg.level_shift), acc, int(cfg.diis_size), int(cfg.diis_start), float(cfg.diis_damping),
-                    float(cfg.trust_radius), int(bool(cfg.fp32_exchange)), float(cfg.fp32_switch_density),
-                    2 if cfg.mu_method == "newton" else 0, int(bool(cfg.warm_eigh)))
+    project = cfg.project_fn
+    if cfg.fp32_exchange and fock_build_fn is not None:
+        raise ValueError("SCFConfig.fp32_exchange applies to the built-in Fock build, not to a fock_build_fn.")
+    sc = _scf_config_struct(cfg)
     need = C.c_size_t(0)
     _lib.check(L.hf_scf_workspace_size(C.byref(pb), C.byref(sc), C.byref(need)))
     ws = _lib.workspace(need.value, dev, "scf")
     P0d = torch.as_tensor(P0).to(dev, cd).contiguous()
     density = torch.empty_like(P0d)
     fock = torch.empty_like(P0d)
+    errors = []
+    if fock_build_fn is not None or project is not None:
+        nk1, nk2, nb = kernel.shape
+        shape = (nk1, nk2, nb, nb)
+        view = _buffer_views(ws, density, fock)
+        fkw = kc.fock_kwargs()
+        ops_L, s_ptr = _lib.lib(), _lib.stream_ptr(dev)
+
+        def fock_cb(user, stream, Pp, Sp, Hp, Fp):
+            try:
+                Sg, Hh, Fn = fock_build_fn(view(Pp, shape), project_fn=None, **fkw)
+                view(Sp, shape).copy_(Sg)
+                Hh = torch.as_tensor(Hh).to(dev, cd)
+                view(Hp, (nb, nb)).copy_(Hh.reshape(-1, nb, nb)[0] if Hh.numel() >= nb * nb else Hh.expand(nb, nb))
+                view(Fp, shape).copy_(Fn)
+                return 0
+            except Exception as exc:  # re-raised after the C call returns
+                errors.append(exc)
+                return _lib.HF_ERR_ABORTED
+
+        def project_cb(user, stream, Xp):
+            try:
+                X = view(Xp, shape)
+                Y = torch.as_tensor(project(X)).to(dev, cd).contiguous()
+                _lib.check(ops_L.hf_axpby(s_ptr, nk1 * nk2, nb, 1.0, Y.data_ptr(), 0.0, None, 1, X.data_ptr()))
+                return 0
+            except Exception as exc:
+                errors.append(exc)
+                return _lib.HF_ERR_ABORTED
+
+        sc.fock_cb = FOCK_CB(fock_cb) if fock_build_fn is not None else FOCK_CB()
+        sc.project_cb = PROJECT_CB(project_cb) if project is not None else PROJECT_CB()
     m = int(cfg.max_iter)
     hist = np.zeros((3, m))
     out = np.full(5, -1.0)
     dp = lambda a: a.ctypes.data_as(C.c_void_p)
-    _lib.check(L.hf_scf_solve(_lib.stream_ptr(dev), C.byref(pb), C.byref(sc), P0d.data_ptr(), density.data_ptr(),
-                              fock.data_ptr(), dp(hist[0]), dp(hist[1]), dp(hist[2]), dp(out), ws.data_ptr(),
-                              ws.numel()))
+    st = L.hf_scf_solve(_lib.stream_ptr(dev), C.byref(pb), C.byref(sc), P0d.data_ptr(), density.data_ptr(),
+                        fock.data_ptr(), dp(hist[0]), dp(hist[1]), dp(hist[2]), dp(out), ws.data_ptr(), ws.numel())
+    if errors:
+        raise errors[0]
+    _lib.check(st)
     n_iter = int(out[2])
     converged = bool(out[3] != 0.0)
     hE, hD, hC = hist[0, :n_iter].copy(), hist[1, :n_iter].copy(), hist[2, :n_iter].copy()
@@ -372,7 +431,7 @@ def _scf_batch_item_type():
 
 def _scf_config_struct(cfg):
     acc = {"linear": 0, "diis": 1, "oda": 2}[cfg.acceleration]
-    return _ScfConfig(int(cfg.max_iter), float(cfg.density_tol), float(cfg.comm_tol), float(cfg.mixing),
+    return _scf_config_type()(int(cfg.max_iter), float(cfg.density_tol), float(cfg.comm_tol), float(cfg.mixing),
                       float(cfg.level_shift), acc, int(cfg.diis_size), int(cfg.diis_start), float(cfg.diis_damping),
                       float(cfg.trust_radius), int(bool(cfg.fp32_exchange)), float(cfg.fp32_switch_density),
                       2 if cfg.mu_method == "newton" else 0, int(bool(cfg.warm_eigh)))

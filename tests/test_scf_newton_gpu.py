@@ -173,6 +173,47 @@ def test_gram_row_matches_gram(cuda, n):
                          ws.data_ptr()) == _lib.HF_ERR_INVALID
 
 
+def test_scf_hooks_in_native_driver_match_python_loop(cuda, monkeypatch):
+    """project_fn (a symmetry projector) and a custom fock_build_fn run as host callbacks of
+    hf_scf_solve: the same steps as the Python loop, and the projected solve matches the oracle."""
+    from jax_hf_b200 import reference_scf
+    from jax_hf_b200.fock import build_fock
+    from jax_hf_b200.reference_scf import SCFConfig, solve_scf
+    from jax_hf_b200.symmetry import make_project_fn
+    kw = _multiband(nk=6, nb=4)
+    K, Ko = _kernels(kw)
+    ZN = np.diag([1.0, 1.0, -1.0, -1.0]).astype(complex)
+    G2 = np.stack([np.eye(4, dtype=complex), ZN])
+    proj = make_project_fn(unitary_group=G2)
+    proj_o = O.make_project_fn(unitary_group=G2)
+    calls = []
+
+    def my_build(P, **kw2):
+        calls.append(1)
+        return build_fock(P, **kw2)
+
+    P0 = torch.zeros(np.asarray(kw["hamiltonian"]).shape, dtype=torch.complex128, device="cuda")
+    for cfg in (dict(acceleration="diis", max_iter=200), dict(acceleration="linear", mixing=0.5, max_iter=300),
+                dict(acceleration="oda", max_iter=300), dict(acceleration="diis", trust_radius=0.3, max_iter=300)):
+        res = {}
+        for native in (True, False):
+            monkeypatch.setattr(reference_scf, "USE_NATIVE", native)
+            res[native] = solve_scf(K, P0, 30.0, config=SCFConfig(project_fn=proj, **cfg), fock_build_fn=my_build)
+        a, b = res[True], res[False]
+        assert a.converged == b.converged
+        assert abs(a.iterations - b.iterations) <= (3 if cfg["acceleration"] == "diis" else 0)
+        assert abs(float(a.energy) - float(b.energy)) <= 1e-10 * max(1.0, abs(float(b.energy)))
+        assert float((a.density_matrix - b.density_matrix).abs().max()) < 1e-5
+    assert len(calls) > 0
+    monkeypatch.setattr(reference_scf, "USE_NATIVE", True)
+    r = solve_scf(K, P0, 30.0, config=SCFConfig(acceleration="diis", project_fn=proj))
+    ro = O.solve_scf(Ko, np.zeros_like(np.asarray(kw["hamiltonian"], complex)), 30.0,
+                     config=O.SCFConfig(acceleration="diis", project_fn=proj_o))
+    assert r.converged == ro["converged"]
+    assert abs(float(r.energy) - ro["energy"]) <= 1e-9 * max(1.0, abs(ro["energy"]))
+    assert np.abs(r.density_matrix.cpu().numpy() - ro["density_matrix"]).max() < 1e-5
+
+
 def test_scf_config_validation():
     from jax_hf_b200.reference_scf import SCFConfig
     with pytest.raises(ValueError, match="acceleration"):
