@@ -561,16 +561,19 @@ __device__ __forceinline__ void jacobi_smem_cols(double2* SA, double2* SV, doubl
       if (on && isq) {
         const int p = partner;
         const double2 apq = SA[p * LP + c];
-        const double mag = hypot(apq.x, apq.y);
+        // the rotation with four long-latency FP64 operations on its dependent chain:
+        // 1/|a_pq| by rsqrt, t by one sqrt and one divide, cos = rsqrt(1 + t^2)
+        const double r2 = apq.x * apq.x + apq.y * apq.y;
         double cc = 1.0, act = 0.0;
         double2 sp = make_double2(0.0, 0.0);
-        if (mag > thr) {
+        if (r2 > thr * thr) {
+          const double rmag = rsqrt(r2);
           const double app = SA[p * LP + p].x, aqq = SA[c * LP + c].x;
-          const double tau = (aqq - app) / (2.0 * mag);
+          const double tau = 0.5 * (aqq - app) * rmag;
           const double tt = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-          cc = 1.0 / sqrt(1.0 + tt * tt);
-          const double sn = tt * cc;
-          sp = make_double2(sn * apq.x / mag, sn * apq.y / mag);
+          cc = rsqrt(1.0 + tt * tt);
+          const double sr = tt * cc * rmag;
+          sp = make_double2(sr * apq.x, sr * apq.y);
           act = 1.0;
         }
         SP[2 * kk] = make_double2(cc, act);
