@@ -539,6 +539,22 @@ struct JacobiPairs {
   __host__ __device__ static int pb(int t, int k) { return 1 + ((M - 1 - k - 1 + t) % (M - 1)); }
 };
 
+// The rotation that zeroes a_pq (cosine cc, sine sp; act = 1 when it rotates).  A
+// rounding-level change here moves the reference CG's plateau stop on some problems, so
+// both Jacobi variants share this one form.
+__device__ __forceinline__ void jacobi_rotation(double2 apq, double app, double aqq, double thr, double& cc,
+                                                double& act, double2& sp) {
+  const double mag = hypot(apq.x, apq.y);
+  if (mag > thr) {
+    const double tau = (aqq - app) / (2.0 * mag);
+    const double tt = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+    cc = 1.0 / sqrt(1.0 + tt * tt);
+    const double sn = tt * cc;
+    sp = make_double2(sn * apq.x / mag, sn * apq.y / mag);
+    act = 1.0;
+  }
+}
+
 template <int NB>
 __device__ __forceinline__ void jacobi_smem_cols(double2* SA, double2* SV, double2* SP, int c, bool on,
                                                  double thr) {
@@ -561,21 +577,9 @@ __device__ __forceinline__ void jacobi_smem_cols(double2* SA, double2* SV, doubl
       if (on && isq) {
         const int p = partner;
         const double2 apq = SA[p * LP + c];
-        // the rotation with four long-latency FP64 operations on its dependent chain:
-        // 1/|a_pq| by rsqrt, t by one sqrt and one divide, cos = rsqrt(1 + t^2)
-        const double r2 = apq.x * apq.x + apq.y * apq.y;
         double cc = 1.0, act = 0.0;
         double2 sp = make_double2(0.0, 0.0);
-        if (r2 > thr * thr) {
-          const double rmag = rsqrt(r2);
-          const double app = SA[p * LP + p].x, aqq = SA[c * LP + c].x;
-          const double tau = 0.5 * (aqq - app) * rmag;
-          const double tt = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-          cc = rsqrt(1.0 + tt * tt);
-          const double sr = tt * cc * rmag;
-          sp = make_double2(sr * apq.x, sr * apq.y);
-          act = 1.0;
-        }
+        jacobi_rotation(apq, SA[p * LP + p].x, SA[c * LP + c].x, thr, cc, act, sp);
         SP[2 * kk] = make_double2(cc, act);
         SP[2 * kk + 1] = sp;
       }
@@ -628,6 +632,103 @@ __device__ __forceinline__ void jacobi_smem_cols(double2* SA, double2* SV, doubl
         }
       }
       __syncwarp();
+    }
+    if (!__any_sync(0xffffffffu, rotated)) break;
+  }
+}
+
+// The same cyclic Jacobi with each lane's columns of A and V in registers: the partner's
+// column comes by warp shuffles (read before this round's update, consumed row by row),
+// the rotation of every pair is broadcast from the pair's q lane, and the rounds are
+// unrolled so that every row index is a compile-time constant (register arrays are
+// never indexed at run time; the lane's own index selects through compare chains).
+// Same rotations, same order and same exact zeros as jacobi_smem_cols.
+__device__ __forceinline__ double2 shfl2(double2 v, int src) {
+  return make_double2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+}
+
+template <int NB>
+__device__ __forceinline__ void jacobi_reg_cols(double2 (&a)[NB], double2 (&v)[NB], int c, int gb, bool on,
+                                                double thr) {
+  constexpr int M = JacobiPairs<NB>::M, NP = M / 2;
+  if (NB == 1) return;
+  for (int sweep = 0; sweep < 60; ++sweep) {
+    bool rotated = false;
+#pragma unroll
+    for (int t = 0; t < M - 1; ++t) {
+      int partner = -1, kk = -1;
+      bool isq = false;
+#pragma unroll
+      for (int k = 0; k < NP; ++k) {
+        const int a0 = JacobiPairs<NB>::pa(t, k), b0 = JacobiPairs<NB>::pb(t, k);
+        const int p = a0 < b0 ? a0 : b0, q = a0 < b0 ? b0 : a0;
+        if (q < NB) {
+          if (c == p) { partner = q; kk = k; }
+          if (c == q) { partner = p; kk = k; isq = true; }
+        }
+      }
+      const int pl = gb + (partner >= 0 ? partner : (c < NB ? c : 0));
+      double2 own = a[0], apq = a[0];  // a[c] and a[partner], by compare chains
+#pragma unroll
+      for (int r = 1; r < NB; ++r) {
+        if (r == c) own = a[r];
+        if (r == partner) apq = a[r];
+      }
+      const double app = __shfl_sync(0xffffffffu, own.x, pl);  // the partner's diagonal
+      double cc = 1.0, act = 0.0;
+      double2 sp = make_double2(0.0, 0.0);
+      if (on && isq) jacobi_rotation(apq, app, own.x, thr, cc, act, sp);
+      double hc[NP], ha[NP];
+      double2 hs[NP];
+#pragma unroll
+      for (int k = 0; k < NP; ++k) {
+        const int a0 = JacobiPairs<NB>::pa(t, k), b0 = JacobiPairs<NB>::pb(t, k);
+        const int q = a0 < b0 ? b0 : a0;
+        const int src = gb + (q < NB ? q : 0);
+        hc[k] = __shfl_sync(0xffffffffu, cc, src);
+        ha[k] = __shfl_sync(0xffffffffu, act, src);
+        hs[k] = shfl2(sp, src);
+      }
+      double mcc = 1.0, mact = 0.0;
+      double2 msp = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int k = 0; k < NP; ++k)
+        if (k == kk) {
+          mcc = hc[k];
+          mact = ha[k];
+          msp = hs[k];
+        }
+      const bool mix = on && mact != 0.0;
+      rotated = rotated || mix;
+      const double2 beta = isq ? msp : make_double2(-msp.x, msp.y);  // q: sp;  p: -conj(sp)
+      // A <- A G, V <- V G on this lane's column: new = cc own + beta partner
+#pragma unroll
+      for (int r = 0; r < NB; ++r) {
+        const double2 xa = shfl2(a[r], pl), xv = shfl2(v[r], pl);
+        if (mix) {
+          a[r] = cadd(cscale(a[r], mcc), cmul(beta, xa));
+          v[r] = cadd(cscale(v[r], mcc), cmul(beta, xv));
+        }
+      }
+      // A <- G^H A: rows p and q of this lane's column, every active pair; then exact zeros
+      if (on) {
+#pragma unroll
+        for (int k = 0; k < NP; ++k) {
+          const int a0 = JacobiPairs<NB>::pa(t, k), b0 = JacobiPairs<NB>::pb(t, k);
+          const int p = a0 < b0 ? a0 : b0, q = a0 < b0 ? b0 : a0;
+          if (q >= NB || ha[k] == 0.0) continue;
+          const double2 x = a[p], y = a[q];
+          a[p] = csub(cscale(x, hc[k]), cmul(hs[k], y));
+          a[q] = cadd(cmulc(x, hs[k]), cscale(y, hc[k]));
+        }
+        if (mact != 0.0) {
+#pragma unroll
+          for (int r = 0; r < NB; ++r) {
+            if (r == partner) a[r] = make_double2(0.0, 0.0);
+            if (r == c) a[r].y = 0.0;
+          }
+        }
+      }
     }
     if (!__any_sync(0xffffffffu, rotated)) break;
   }
@@ -713,17 +814,35 @@ __device__ __forceinline__ void eig_cols(int nk, const double2* __restrict__ A, 
 #pragma unroll
     for (int off = G / 2; off > 0; off >>= 1) fro += __shfl_xor_sync(0xffffffffu, fro, off);
     __syncwarp();
-    if (on) {
+    double2 vc[NB];  // this lane's column of V, from the identity
 #pragma unroll
-      for (int r = 0; r < NB; ++r) {
-        SA[r * LP + c] = hm[r];
-        SV[r * LP + c] = make_double2(r == c ? 1.0 : 0.0, 0.0);
+    for (int r = 0; r < NB; ++r) vc[r] = make_double2(r == c ? 1.0 : 0.0, 0.0);
+    double wc = 0.0;
+    const double thr = fmax(tol * sqrt(fro), 1e-300);
+    if constexpr (NB <= 4) {
+      // columns in registers (measured on a B200: nb = 4 in 0.70 of the shared-memory time;
+      // from nb = 8 on, the register version spills and its shuffles cost more)
+      jacobi_reg_cols<NB>(hm, vc, c, g * G, on, thr);
+#pragma unroll
+      for (int r = 0; r < NB; ++r)
+        if (r == c) wc = hm[r].x;
+    } else {
+      if (on) {
+#pragma unroll
+        for (int r = 0; r < NB; ++r) {
+          SA[r * LP + c] = hm[r];
+          SV[r * LP + c] = vc[r];
+        }
+      }
+      __syncwarp();
+      jacobi_smem_cols<NB>(SA, SV, SP, c, on, thr);
+      if (on) {
+        wc = SA[c * LP + c].x;
+#pragma unroll
+        for (int r = 0; r < NB; ++r) vc[r] = SV[r * LP + c];
       }
     }
-    __syncwarp();
-    jacobi_smem_cols<NB>(SA, SV, SP, c, on, fmax(tol * sqrt(fro), 1e-300));
     // ascending order: lane c's eigenpair goes to column rank(c)
-    const double wc = on ? SA[c * LP + c].x : 0.0;
     if (on) SW[c] = wc;
     __syncwarp();
     if (on) {
@@ -737,12 +856,12 @@ __device__ __forceinline__ void eig_cols(int nk, const double2* __restrict__ A, 
         for (int r = 0; r < NB; ++r) {
           double2 acc = make_double2(0.0, 0.0);
 #pragma unroll
-          for (int j = 0; j < NB; ++j) acc = cfma(SQ[r * LP + j], SV[j * LP + c], acc);
+          for (int j = 0; j < NB; ++j) acc = cfma(SQ[r * LP + j], vc[j], acc);
           Qout[out + (size_t)r * NB] = acc;
         }
       } else {
 #pragma unroll
-        for (int r = 0; r < NB; ++r) Qout[out + (size_t)r * NB] = SV[r * LP + c];
+        for (int r = 0; r < NB; ++r) Qout[out + (size_t)r * NB] = vc[r];
       }
     }
     __syncwarp();
