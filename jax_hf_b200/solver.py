@@ -372,7 +372,8 @@ def solve_batch(kernels, P0s, n_electrons, *, config: SolverConfig | None = None
     lanes = max(1, min(int(lanes), n))
     times = (C.c_double * n)()
     if graph:
-        ws = _lib.workspace(n * per_lane, dev, "cg_batch")
+        # one workspace per solve, released on return (not kept in the workspace cache)
+        ws = torch.empty(max(n * per_lane, 256), dtype=torch.uint8, device=dev)
         _lib.check(L.hf_cg_solve_batch_graph(_lib.stream_ptr(dev), items, n, C.byref(conf), ws.data_ptr(),
                                              per_lane, times))
     else:
