@@ -59,6 +59,10 @@ class SCFConfig:
     fp32_switch_density: float = 1e-5
     mu_method: str = "bisection"
     warm_eigh: bool = False
+    # an FP64 reference solution (energy, and optionally density) to report the result's
+    # error against: history["rel_dE_vs_reference"], history["max_abs_dP_vs_reference"]
+    reference_energy: float | None = None
+    reference_density: Any = None
 
     def __post_init__(self) -> None:
         if self.max_iter <= 0:
@@ -120,9 +124,22 @@ class _Ops:
 def solve_scf(kernel, P0, n_electrons: float, *, config: SCFConfig | None = None,
               fock_build_fn: Callable | None = None) -> SCFResult:
     """Reference SCF solver (reference_scf.py:124-219)."""
-    if config is None:
-        config = SCFConfig()
-    cfg = config
+    cfg = config if config is not None else SCFConfig()
+    return _reference_errors(_solve_scf_impl(kernel, P0, n_electrons, cfg, fock_build_fn), cfg)
+
+
+def _reference_errors(r: SCFResult, cfg: SCFConfig) -> SCFResult:
+    """Adds the result's error against a supplied FP64 reference to its history."""
+    if cfg.reference_energy is not None:
+        Er = float(cfg.reference_energy)
+        r.history["rel_dE_vs_reference"] = abs(float(r.energy) - Er) / max(abs(Er), 1e-300)
+    if cfg.reference_density is not None:
+        Pr = torch.as_tensor(cfg.reference_density).to(r.density_matrix.device, r.density_matrix.dtype)
+        r.history["max_abs_dP_vs_reference"] = float((r.density_matrix - Pr).abs().max())
+    return r
+
+
+def _solve_scf_impl(kernel, P0, n_electrons, cfg, fock_build_fn):
     dev = kernel.device
     nk1, nk2, nb = kernel.shape
     cd = torch.complex128
@@ -518,6 +535,7 @@ class ScfScanGraph:
                 iterations=n_iter, converged=converged, message=message,
                 history={"E": h[0].copy(), "density_residual": h[1].copy(), "commutator_residual": h[2].copy(),
                          "fp32_switch_iter": int(o[4]) if self.cfg.fp32_exchange else -1}))
+        results = [_reference_errors(r, self.cfg) for r in results]
         return (results, list(times)) if return_times else results
 
     def close(self):

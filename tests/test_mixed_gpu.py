@@ -63,6 +63,11 @@ def test_fast_scf_reaches_the_oracle_fixed_point(cuda, name, kw, ne, fp32):
         assert r.history["fp32_switch_iter"] >= 1
     else:
         assert r.history["fp32_switch_iter"] == -1
+    # the same solve reporting its error against the oracle's fixed point
+    r2 = solve_scf(K, P0, ne, config=SCFConfig(**FAST, fp32_exchange=fp32, reference_energy=Eo,
+                                               reference_density=ro["density_matrix"]))
+    assert r2.history["rel_dE_vs_reference"] <= TOL_E
+    assert r2.history["max_abs_dP_vs_reference"] < TOL_P
 
 
 @pytest.mark.parametrize("name,kw,ne", CASES[:2], ids=[c[0] for c in CASES[:2]])
