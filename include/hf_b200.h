@@ -257,7 +257,12 @@ int hf_free_energy(void* stream, int dtype, int nk1, int nk2, int nb, const doub
  * maxiter <= 0 picks the reference default for the method and dtype.
  * weights: method 0/1 take raw weights and n_electrons; method 2 takes the
  * normalised weights and n_target_norm (as the solver does).  mu0 (device,
- * float64) is read by method 2 only.  mu_out is a float64 device scalar.
+ * float64, may be NULL) is method 2's warm start and, for method 0, a hint (a
+ * previous mu): Newton passes from it certify a bracket around the root, and
+ * the bisection levels whose midpoints lie outside it are decided without
+ * evaluations, with the decisions, and so the result, of evaluating every
+ * level; method 1 ignores it.  mu0 may alias mu_out.  mu_out is a float64
+ * device scalar.
  */
 int hf_find_mu(void* stream, int dtype, int method, int nk1, int nk2, int nb, const void* eps,
                const void* weights, double n_electrons, double T, int maxiter, const double* mu0,

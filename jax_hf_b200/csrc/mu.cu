@@ -6,8 +6,13 @@
 // through distributed shared memory and reduces them with a fixed shuffle tree.
 // All CTAs therefore hold bit-identical (mu, lo, hi) and take identical
 // branches; no global-memory round trip and no second launch per iteration.
-// The bisection evaluates four levels per pass (the 15 midpoints of the next
-// four levels in one reduction, then the four decisions in order).
+// The bisection evaluates two levels per pass (the 3 midpoints of the next two
+// levels in one reduction, then the two decisions in order).  Each pass costs a
+// chain of block and cluster reductions whose latency grows with the number of
+// sums: on 2304 eigenvalues (9 CTAs) the 54 steps take 52 us at two levels per
+// pass (27 passes), 59 us at three, 65 us at one and 91 us at four; storing the
+// warp partials into every CTA's shared memory behind a single cluster barrier
+// instead of the two-stage reduction measured slower (63 us at two levels).
 //
 // Methods (reference):
 //   0  _find_mu_bisection  utils.py:353-382 (maxiter 54 f64 / 30 f32)
@@ -32,7 +37,8 @@ namespace hf {
 
 constexpr int kMuThreads = 1024;
 constexpr int kMuMaxCluster = 16;  // non-portable size, used when the device schedules it
-constexpr int kBisLevels = 4;  // bisection levels per pass of the 256-thread variant
+constexpr int kBisLevels = 2;  // bisection levels per pass of the 256-thread variant
+constexpr int kMuCertPasses = 6;  // Newton passes of a hinted bisection (certified bracket)
 
 struct MuArgs {
   const void* eps;
@@ -192,7 +198,7 @@ __device__ __forceinline__ void cluster_minmax(cg::cluster_group& cl, double& mn
 
 __device__ __forceinline__ double expit(double x) { return 1.0 / (1.0 + exp(-x)); }
 
-// BT threads per CTA; the bisection evaluates L levels per pass (L = 4 for the
+// BT threads per CTA; the bisection evaluates L levels per pass (L = 2 for the
 // 256-thread variant, 1 for the 1024-thread variant, whose register budget is 64).
 template <typename RT, int BT>
 __global__ void __launch_bounds__(BT) k_find_mu(const MuArgs a) {
@@ -203,6 +209,8 @@ __global__ void __launch_bounds__(BT) k_find_mu(const MuArgs a) {
   __shared__ double wsm[66];
   __shared__ double bslots[2][NODES];
   __shared__ double bsm[33 * NODES];
+  __shared__ double cslots[2][5];  // the certifying Newton passes of a hinted bisection
+  __shared__ double csm[33 * 5];
   extern __shared__ double2 mu_cache[];  // a.cache: (eps, w) of this thread's elements, [u][thread]
   const int gt = cl.block_rank() * blockDim.x + threadIdx.x;
   const int gs = cl.num_blocks() * blockDim.x;
@@ -229,6 +237,9 @@ __global__ void __launch_bounds__(BT) k_find_mu(const MuArgs a) {
     }
   };
 
+  // method 0 with a hint (the caller's previous mu): read before any CTA can write a.out
+  const double hint = (a.method == 0 && a.mu0 != nullptr) ? a.mu0[0] : 0.0;
+  const bool has_hint = a.method == 0 && a.mu0 != nullptr && isfinite(hint);
   // Method 2 with a warm start: the min/max pass also forms N and Z at mu0, which
   // are the first Newton evaluation whenever mu0 lies inside the bracket.
   const bool fuse_first = a.method == 2 && a.mu0 != nullptr;
@@ -269,6 +280,63 @@ __global__ void __launch_bounds__(BT) k_find_mu(const MuArgs a) {
     const double Td = T + 1e-12, iTd = 1.0 / Td;
     int it = 0;
     bool fixed = false;
+    if (has_hint) {
+      // Certified bracket from the hint.  N(x) = sum w / (1 + exp((e - x) / Td)) is
+      // increasing in x; an evaluation N~(x) differs from it by at most E = (kpt + 24) u W
+      // (kpt terms summed per thread, a reduction tree of depth <= 14, about 6 u per term
+      // and u W for the rounding of the exponent's argument; W = sum w).  So once
+      // N~(A) > target + margin with margin = 8 (kpt + 24) u W >= 2E, every x >= A has
+      // N~(x) > target: the bisection's decision at a midpoint m >= A is "above" without
+      // an evaluation, and likewise "below" for m <= B once N~(B) < target - margin.
+      // Newton passes from the hint put A and B within a few margin / N' of the root,
+      // each evaluating N and N' at the iterate and N at two probes around it; then the
+      // levels whose midpoints lie outside (B, A) are replayed without evaluations and
+      // only the last few levels are evaluated.  The decisions, and so the result, are
+      // those of evaluating every level.
+      const int kpt = (a.n + gs - 1) / gs;
+      double A = INFINITY, B = -INFINITY;
+      double m = fmin(fmax(hint, lo), hi), d = 0.0;
+      for (int t = 0; t < kMuCertPasses; ++t) {
+        const double pl = m - d, ph = m + d;
+        double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // N(m), N'(m) Td, N(pl), N(ph), W
+        visit([&](double ev, double w) {
+          const double f = 1.0 / (1.0 + exp((ev - m) * iTd));
+          v[0] += w * f;
+          v[1] += w * (f * (1.0 - f));
+          v[2] += w / (1.0 + exp((ev - pl) * iTd));
+          v[3] += w / (1.0 + exp((ev - ph) * iTd));
+          v[4] += w;
+        });
+        cluster_sum_n<5>(cl, v, cslots, csm, parity);
+        parity ^= 1;
+        const double margin = 8.0 * (kpt + 24) * 1.1102230246251565e-16 * v[4];
+        const double xs[3] = {m, pl, ph}, ns[3] = {v[0], v[2], v[3]};
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          if (ns[q] > a.target + margin) A = fmin(A, xs[q]);
+          if (ns[q] < a.target - margin) B = fmax(B, xs[q]);
+        }
+        const double Z = v[1] * iTd;
+        const double bl = fmax(B, lo), bh = fmin(A, hi);
+        double r = m - (v[0] - a.target) / Z;
+        if (!(Z > 0.0) || !isfinite(r) || r <= bl || r >= bh) r = 0.5 * (bl + bh);
+        const double floor_w = Z > 0.0 ? 2.0 * margin / Z : INFINITY;
+        if (A - B <= 4.0 * floor_w) break;  // as narrow as the margin allows
+        d = fmax(2.0 * fabs(r - m), floor_w);
+        m = r;
+      }
+      while (it < a.maxiter) {  // the levels decided by the certified bracket
+        const double mid = 0.5 * (lo + hi);
+        double nl, nh;
+        if (mid >= A) { nl = lo; nh = mid; }
+        else if (mid <= B) { nl = mid; nh = hi; }
+        else break;
+        if (nl == lo && nh == hi) { fixed = true; break; }
+        lo = nl;
+        hi = nh;
+        ++it;
+      }
+    }
     while (it < a.maxiter && !fixed) {
       double nlo[NODES + 1], nhi[NODES + 1], mid[NODES + 1];
       nlo[1] = lo;
@@ -429,7 +497,7 @@ int hf::find_mu_internal(void* stream, int dtype, int method, int nk1, int nk2, 
   a.eps = eps; a.w = weights;
   a.n = (int)n_all; a.nb = nb; a.method = method; a.maxiter = maxiter;
   a.target = n_electrons; a.T = T; a.mu0 = mu0; a.out = mu_out; a.active = active;
-  // bisection: every pass evaluates 15 midpoints per eigenvalue, so small
+  // bisection: every pass evaluates 3 midpoints per eigenvalue, so small
   // meshes use 256-thread CTAs with one eigenvalue per thread, spread over up to 16
   // SMs; the Newton variants (one evaluation per pass, bound by the cluster barrier
   // of each pass): up to four per thread of 1024-thread CTAs

@@ -115,7 +115,7 @@ struct Scf {
     return hf_axpby(s, (size_t)nk, nb, a, x, b, y, 1, out);
   }
   bool fp32 = false;    // this build runs the exchange FFT in FP32
-  bool mu_warm = false;  // mu from the Newton-bracket solver started at the previous mu
+  bool mu_warm = false;  // a previous mu exists: the Newton-bracket start, or the bisection's hint
   bool eig_warm = false; // eigh started from the eigenvectors in kV (the previous decomposition)
   bool eig_cols = false; // eigh by the lane-per-column Jacobi (warm_eigh mode, nb <= 8)
   // herm(project(X)) in place (the caller's projector), or nothing without one
@@ -160,7 +160,9 @@ struct Scf {
       return st;
     }
     // mu_method 2: Newton-bracket solver, from mu = 0 in the first call and from the previous
-    // mu afterwards (the warm start reads that word before the kernel overwrites it)
+    // mu afterwards; mu_method 0: the bisection, given the previous mu as a hint that decides
+    // most levels without evaluations (same result).  The kernel reads that word before it
+    // overwrites it.
     if ((st = hf_find_mu(s, HF_C128, cf->mu_method == 2 ? 2 : 0, nk, 1, nb, at<double>(kEV), pb->w2d,
                          pb->n_electrons, pb->T, 0, mu_warm ? sc + kSMuRaw : nullptr, sc + kSMuRaw)))
       return st;
@@ -171,7 +173,7 @@ struct Scf {
                          at<double>(kSH))))
         return st;
       if ((st = hf_find_mu(s, HF_C128, 0, nk, 1, nb, at<double>(kSH), pb->w2d, pb->n_electrons, pb->T, 0,
-                           nullptr, sc + kSMu)))
+                           mu_warm ? sc + kSMu : nullptr, sc + kSMu)))
         return st;
       shifted = at<double>(kSH);
       mu = sc + kSMu;
@@ -295,7 +297,7 @@ extern "C" int hf_scf_solve(void* stream, const hf_cg_problem* pb, const hf_scf_
         std::fill(Bkeep.begin(), Bkeep.end(), 0.0);
       }
     }
-    S.mu_warm = cf->mu_method == 2 && k > 0;
+    S.mu_warm = k > 0;
     S.eig_cols = cf->warm_eigh != 0 && nb <= 8;
     S.eig_warm = S.eig_cols && k > 0;
     if ((st = S.build_and_occupy(density, F, Pn))) return st;
@@ -388,7 +390,7 @@ extern "C" int hf_scf_solve(void* stream, const hf_cg_problem* pb, const hf_scf_
   }
   // final build at the returned density (reference_scf.py:345-347), FP64 in every mode
   S.fp32 = false;
-  S.mu_warm = cf->mu_method == 2 && k > 0;
+  S.mu_warm = k > 0;
   S.eig_cols = cf->warm_eigh != 0 && nb <= 8;
   S.eig_warm = S.eig_cols && k > 0;
   if ((st = S.build_and_occupy(density, fock, S.at<void>(kPN)))) return st;
@@ -606,7 +608,7 @@ int scf_iteration_dev(Scf& S, Capture& cap, cudaGraph_t g, std::vector<cudaGraph
   k_scf_dev_iter_begin<<<1, 1, 0, cap.s>>>(d, nh);
   HF_LAUNCH_CHECK("k_scf_dev_iter_begin");
   S.fp32 = fp32_phase;
-  S.mu_warm = cf->mu_method == 2 && warm;
+  S.mu_warm = warm;
   S.eig_cols = cf->warm_eigh != 0 && nb <= 8;
   S.eig_warm = S.eig_cols && warm;
   if ((st = S.build_and_occupy(density, F, Pn))) return st;
@@ -804,7 +806,7 @@ extern "C" int hf_scf_batch_graph_create(const hf_scf_batch_item* items, int n_i
       // final build at the returned density, FP64 (reference_scf.py:345-347)
       if ((e = cap.into(G, tail))) return e;
       S.fp32 = false;
-      S.mu_warm = cf->mu_method == 2 && cf->max_iter > 0;
+      S.mu_warm = cf->max_iter > 0;
       S.eig_cols = cf->warm_eigh != 0 && S.nb <= 8;
       S.eig_warm = S.eig_cols && cf->max_iter > 0;
       HF_CUDA(cudaMemcpyAsync(it.density, S.at<void>(kPD), qbytes, cudaMemcpyDeviceToDevice, cap.s));

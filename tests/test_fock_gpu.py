@@ -209,6 +209,52 @@ def test_find_mu(cuda, method, T):
     assert abs(mu - muo) < 1e-9 * max(1.0, abs(muo)) or T < 1e-3
 
 
+@pytest.mark.parametrize("shape,T,kind", [((24, 24, 4), 0.1, "metal"), ((36, 36, 6), 0.05, "metal"),
+                                          ((16, 16, 4), 0.01, "gapped"), ((12, 12, 3), 0.0, "metal"),
+                                          ((96, 96, 4), 0.1, "metal")])
+def test_bisection_hint_keeps_the_result(cuda, shape, T, kind):
+    """hf_find_mu method 0 with a hint (mu0) decides the levels outside a certified
+    bracket without evaluations; the result must be bit-identical to evaluating every
+    level, for good, poor and useless hints, metals and a gapped spectrum."""
+    from jax_hf_b200 import _lib
+    rng = np.random.default_rng(7)
+    nk1, nk2, nb = shape
+    if kind == "gapped":
+        lower = rng.uniform(-4, -1, (nk1, nk2, nb // 2))
+        bands = np.concatenate([lower, rng.uniform(1, 4, (nk1, nk2, nb - nb // 2))], axis=-1)
+        ne = float(nb // 2)
+    else:
+        bands = rng.standard_normal(shape) * 2
+        ne = 0.4 * nb
+    eps = torch.as_tensor(bands, device="cuda")
+    w = torch.full((nk1, nk2), 1.0 / (nk1 * nk2), device="cuda", dtype=torch.float64)
+    out = torch.zeros(1, device="cuda", dtype=torch.float64)
+    L = _lib.lib()
+    st = _lib.stream_ptr(eps.device)
+
+    def run(hint):
+        h = None
+        if hint is not None:
+            h = torch.tensor([hint], device="cuda", dtype=torch.float64)
+        _lib.check(L.hf_find_mu(st, 0, 0, nk1, nk2, nb, eps.data_ptr(), w.data_ptr(), ne, T, 0,
+                                None if h is None else h.data_ptr(), out.data_ptr()))
+        return float(out.item())
+
+    ref = run(None)
+    if kind == "metal" and T >= 1e-3:
+        # inside a gap the count is flat to rounding, and where the bisection stops there
+        # depends on the summation order: only a metal's mu is compared with the oracle
+        muo = O.find_chemical_potential(bands, w.cpu().numpy(), ne, T, method="bisection")
+        assert abs(ref - muo) < 1e-9 * max(1.0, abs(muo))
+    for hint in (ref, ref + 1e-9, ref - 1e-3, ref + 0.3, 0.0, 1e6, -50.0, float("nan")):
+        assert run(hint) == ref, hint
+    # the hint may alias the output (the SCF driver passes its previous mu in place)
+    out.fill_(ref + 1e-6)
+    _lib.check(L.hf_find_mu(st, 0, 0, nk1, nk2, nb, eps.data_ptr(), w.data_ptr(), ne, T, 0,
+                            out.data_ptr(), out.data_ptr()))
+    assert float(out.item()) == ref
+
+
 def test_solve_mu_warm_start(cuda):
     from jax_hf_b200.utils import solve_mu
     rng = np.random.default_rng(1)
