@@ -48,10 +48,13 @@ struct MuArgs {
   const double* mu0;
   double* out;
   const int* active;  // optional device flag: return at once when *active == 0
-  int cache;          // n <= 4 x threads of the cluster: (eps, w) kept in shared memory
+  int cache;          // elements per thread kept in shared memory as (eps, w); 0: read from L2
 };
-// (eps, w) entries of one thread in the shared-memory cache (layout [u][thread])
+// loads in flight per thread when the elements are read from L2
 constexpr int kMuCacheU = 4;
+// the shared-memory cache holds up to this many (eps, w) entries per thread (layout
+// [u][thread]; 192 KB for 1024 threads): a 144 x 144 x 8 spectrum on 16 CTAs needs 11
+constexpr int kMuCacheMax = 12;
 
 template <typename RT>
 __device__ __forceinline__ double load_eps(const MuArgs& a, int e) {
@@ -198,9 +201,28 @@ __device__ __forceinline__ void cluster_minmax(cg::cluster_group& cl, double& mn
 
 __device__ __forceinline__ double expit(double x) { return 1.0 / (1.0 + exp(-x)); }
 
+// x / b, correctly rounded, for a divisor b fixed over a pass with rb = 1 / b (correctly
+// rounded).  q0 = x rb is within 1.5 ulp of x / b; one fma remainder step x - q0 b and
+// correction makes it faithful, and by Markstein's theorem (P. Markstein, IBM J. Res.
+// Dev. 34 (1990) 111-119: with y the correctly rounded 1/b and q faithful, r = x - q b is
+// exact under an fma and q + r y rounds to the correctly rounded x / b) a second step
+// gives the correctly rounded quotient, the bits of x / b.  The remainder must not
+// underflow, so numerators below 2^-900 in magnitude (and NaN) take the division.
+// Five fp64 operations in place of a division routine per element, at the same bits.
+__device__ __forceinline__ double div_by(double x, double b, double rb) {
+  if (!(fabs(x) >= 0x1p-900)) return x / b;
+  double q = x * rb;
+  double r = fma(-q, b, x);
+  q = fma(r, rb, q);
+  r = fma(-q, b, x);
+  return fma(r, rb, q);
+}
+
 // BT threads per CTA; the bisection evaluates L levels per pass (L = 2 for the
 // 256-thread variant, 1 for the 1024-thread variant, whose register budget is 64).
-template <typename RT, int BT>
+// NEWTON: methods 1 and 2 only (1024 threads); otherwise the bisection only, so that
+// neither variant carries the other's registers (1024-thread CTAs have 64 per thread).
+template <typename RT, int BT, bool NEWTON>
 __global__ void __launch_bounds__(BT) k_find_mu(const MuArgs a) {
   constexpr int L = BT <= 256 ? kBisLevels : 1, NODES = (1 << L) - 1;
   if (a.active && !*a.active) return;  // uniform across the cluster: no barrier is skipped by a subset
@@ -217,17 +239,15 @@ __global__ void __launch_bounds__(BT) k_find_mu(const MuArgs a) {
   // every pass visits this thread's elements in the same order, from shared memory when
   // they fit (each thread reads back only what it stored: no barrier), else from L2
   if (a.cache) {
-#pragma unroll
-    for (int u = 0; u < kMuCacheU; ++u) {
+    for (int u = 0; u < a.cache; ++u) {
       const int e = gt + u * gs;
       mu_cache[u * blockDim.x + threadIdx.x] =
           e < a.n ? make_double2(load_eps<RT>(a, e), load_w<RT>(a, e)) : make_double2(0.0, 0.0);
     }
   }
   auto visit = [&](auto&& f) {
-    if (a.cache) {
-#pragma unroll
-      for (int u = 0; u < kMuCacheU; ++u)
+    if (a.cache) {  // the same elements in the same order as the L2 path
+      for (int u = 0; u < a.cache; ++u)
         if (gt + u * gs < a.n) {
           const double2 c = mu_cache[u * blockDim.x + threadIdx.x];
           f(c.x, c.y);
@@ -238,21 +258,21 @@ __global__ void __launch_bounds__(BT) k_find_mu(const MuArgs a) {
   };
 
   // method 0 with a hint (the caller's previous mu): read before any CTA can write a.out
-  const double hint = (a.method == 0 && a.mu0 != nullptr) ? a.mu0[0] : 0.0;
-  const bool has_hint = a.method == 0 && a.mu0 != nullptr && isfinite(hint);
+  const double hint = (!NEWTON && a.mu0 != nullptr) ? a.mu0[0] : 0.0;
+  const bool has_hint = !NEWTON && a.mu0 != nullptr && isfinite(hint);
   // Method 2 with a warm start: the min/max pass also forms N and Z at mu0, which
   // are the first Newton evaluation whenever mu0 lies inside the bracket.
-  const bool fuse_first = a.method == 2 && a.mu0 != nullptr;
+  const bool fuse_first = NEWTON && a.method == 2 && a.mu0 != nullptr;
   const double mu0v = fuse_first ? a.mu0[0] : 0.0;
-  const double Tf = fmax(a.T, 1e-12);
+  const double Tf = fmax(a.T, 1e-12), rTf = 1.0 / Tf;
   double mn = INFINITY, mx = -INFINITY, N0 = 0.0, Z0 = 0.0;
   if (fuse_first) {
     visit([&](double v, double w) {
       mn = fmin(mn, v);
       mx = fmax(mx, v);
-      const double p = expit((mu0v - v) / Tf);
+      const double p = expit(div_by(mu0v - v, Tf, rTf));
       N0 += w * p;
-      Z0 += w * (p * (1.0 - p)) / Tf;
+      Z0 += div_by(w * (p * (1.0 - p)), Tf, rTf);
     });
   } else {
     visit([&](double v, double) {
@@ -268,7 +288,7 @@ __global__ void __launch_bounds__(BT) k_find_mu(const MuArgs a) {
   }
 
   double result;
-  if (a.method == 0) {
+  if constexpr (!NEWTON) {
     // L levels of the bisection per pass: the counts at all 2^L - 1
     // midpoints of the next L levels (a binary tree of intervals, each midpoint
     // formed exactly as the one-level loop would form it) come from one cluster
@@ -407,7 +427,7 @@ __global__ void __launch_bounds__(BT) k_find_mu(const MuArgs a) {
     }
     result = 0.5 * (lo + hi);
   } else {
-    const double Tj = fmax(a.T, 1e-12);
+    const double Tj = fmax(a.T, 1e-12), rTj = 1.0 / Tj;
     double lo, hi, mu;
     if (a.method == 1) {
       const double span = mx - mn + 10.0 * fmax(Tj, 1e-6);
@@ -428,9 +448,9 @@ __global__ void __launch_bounds__(BT) k_find_mu(const MuArgs a) {
         Z = Z0;
       } else {
         visit([&](double ev, double w) {
-          const double p = expit((mu - ev) / Tj);
+          const double p = expit(div_by(mu - ev, Tj, rTj));
           N += w * p;
-          Z += w * (p * (1.0 - p)) / Tj;
+          Z += div_by(w * (p * (1.0 - p)), Tj, rTj);
         });
         cluster_sum2(cl, N, Z, slots, wsm, parity);
         parity ^= 1;
@@ -450,7 +470,7 @@ __global__ void __launch_bounds__(BT) k_find_mu(const MuArgs a) {
     }
     if (a.method == 1) {
       double N = 0.0, dummy = 0.0;
-      visit([&](double ev, double w) { N += w * expit((mu - ev) / Tj); });
+      visit([&](double ev, double w) { N += w * expit(div_by(mu - ev, Tj, rTj)); });
       cluster_sum2(cl, N, dummy, slots, wsm, parity);
       parity ^= 1;
       if (fabs(N - a.target) > 1e-12) mu = 0.5 * (lo + hi);
@@ -506,9 +526,12 @@ int hf::find_mu_internal(void* stream, int dtype, int method, int nk1, int nk2, 
   int csize = (a.n + per_cta - 1) / per_cta;
   if (csize < 1) csize = 1;
   if (csize > kMuMaxCluster) csize = kMuMaxCluster;
-  const void* fn = threads == 256 ? (single ? (const void*)k_find_mu<float, 256> : (const void*)k_find_mu<double, 256>)
-                                  : (single ? (const void*)k_find_mu<float, kMuThreads>
-                                            : (const void*)k_find_mu<double, kMuThreads>);
+  const void* fn = method != 0 ? (single ? (const void*)k_find_mu<float, kMuThreads, true>
+                                         : (const void*)k_find_mu<double, kMuThreads, true>)
+                   : threads == 256 ? (single ? (const void*)k_find_mu<float, 256, false>
+                                              : (const void*)k_find_mu<double, 256, false>)
+                                    : (single ? (const void*)k_find_mu<float, kMuThreads, false>
+                                              : (const void*)k_find_mu<double, kMuThreads, false>);
   unsigned long long ctx = 0;
   if (int cst = context_id(&ctx)) return cst;
   // per (kernel, context), set up once under a lock: the largest schedulable cluster
@@ -538,13 +561,16 @@ int hf::find_mu_internal(void* stream, int dtype, int method, int nk1, int nk2, 
       }
       cudaGetLastError();  // a refused query leaves the portable size
       HF_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)((size_t)kMuCacheU * kMuThreads * sizeof(double2))));
+                                   (int)((size_t)kMuCacheMax * kMuThreads * sizeof(double2))));
       it = max_cluster.emplace(key, mc).first;
     }
     if (csize > it->second) csize = it->second;
   }
-  a.cache = a.n <= kMuCacheU * csize * threads ? 1 : 0;
-  const size_t cache_bytes = (size_t)kMuCacheU * threads * sizeof(double2);
+  {
+    const long long per = ((long long)a.n + (long long)csize * threads - 1) / ((long long)csize * threads);
+    a.cache = per <= kMuCacheMax ? (int)per : 0;
+  }
+  const size_t cache_bytes = (size_t)a.cache * threads * sizeof(double2);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(csize, 1, 1);
   cfg.blockDim = dim3(threads, 1, 1);
@@ -557,12 +583,15 @@ int hf::find_mu_internal(void* stream, int dtype, int method, int nk1, int nk2, 
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  if (threads == 256) {
-    if (single) HF_CUDA(cudaLaunchKernelEx(&cfg, k_find_mu<float, 256>, a));
-    else HF_CUDA(cudaLaunchKernelEx(&cfg, k_find_mu<double, 256>, a));
+  if (method != 0) {
+    if (single) HF_CUDA(cudaLaunchKernelEx(&cfg, k_find_mu<float, kMuThreads, true>, a));
+    else HF_CUDA(cudaLaunchKernelEx(&cfg, k_find_mu<double, kMuThreads, true>, a));
+  } else if (threads == 256) {
+    if (single) HF_CUDA(cudaLaunchKernelEx(&cfg, k_find_mu<float, 256, false>, a));
+    else HF_CUDA(cudaLaunchKernelEx(&cfg, k_find_mu<double, 256, false>, a));
   } else {
-    if (single) HF_CUDA(cudaLaunchKernelEx(&cfg, k_find_mu<float, kMuThreads>, a));
-    else HF_CUDA(cudaLaunchKernelEx(&cfg, k_find_mu<double, kMuThreads>, a));
+    if (single) HF_CUDA(cudaLaunchKernelEx(&cfg, k_find_mu<float, kMuThreads, false>, a));
+    else HF_CUDA(cudaLaunchKernelEx(&cfg, k_find_mu<double, kMuThreads, false>, a));
   }
   return HF_OK;
 }
