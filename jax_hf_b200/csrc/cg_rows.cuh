@@ -595,22 +595,26 @@ __device__ __forceinline__ void jacobi_smem_cols(double2* SA, double2* SV, doubl
       }
       rotated = rotated || (on && act != 0.0);
       const double2 beta = isq ? sp : make_double2(-sp.x, sp.y);  // q: sp;  p: -conj(sp)
-      double2 na[NB], nv[NB];
+      // the new columns of A, then of V, each read whole before any lane writes (two
+      // phases keep half as many values live: at the 128-register cap of nb 5-8 the
+      // single phase spilled)
+      double2 nc[NB];
       const bool mix = on && act != 0.0;
       if (mix) {
 #pragma unroll
-        for (int r = 0; r < NB; ++r) {
-          na[r] = cadd(cscale(SA[r * LP + c], cc), cmul(beta, SA[r * LP + partner]));
-          nv[r] = cadd(cscale(SV[r * LP + c], cc), cmul(beta, SV[r * LP + partner]));
-        }
+        for (int r = 0; r < NB; ++r) nc[r] = cadd(cscale(SA[r * LP + c], cc), cmul(beta, SA[r * LP + partner]));
       }
       __syncwarp();
       if (mix) {
 #pragma unroll
-        for (int r = 0; r < NB; ++r) {
-          SA[r * LP + c] = na[r];
-          SV[r * LP + c] = nv[r];
-        }
+        for (int r = 0; r < NB; ++r) SA[r * LP + c] = nc[r];
+#pragma unroll
+        for (int r = 0; r < NB; ++r) nc[r] = cadd(cscale(SV[r * LP + c], cc), cmul(beta, SV[r * LP + partner]));
+      }
+      __syncwarp();
+      if (mix) {
+#pragma unroll
+        for (int r = 0; r < NB; ++r) SV[r * LP + c] = nc[r];
       }
       // A <- G^H A: rows p and q of this lane's column, every active pair; then exact zeros
       if (on) {
