@@ -771,29 +771,29 @@ __device__ __forceinline__ void eig_cols(int nk, const double2* __restrict__ A, 
       }
     }
     if (rotate) {  // SA <- Q^H F Q, column c
-      double2 q[NB], m[NB];
+      // t = A q_c goes through this lane's column of SV (free until V is formed) and
+      // q_c through SQ, so that only one nb-vector is live in registers at a time
       if (on) {
 #pragma unroll
-        for (int r = 0; r < NB; ++r) {
-          q[r] = Qin[base + (size_t)r * NB];
-          SQ[r * LP + c] = q[r];
-        }
+        for (int r = 0; r < NB; ++r) SQ[r * LP + c] = Qin[base + (size_t)r * NB];
       }
       __syncwarp();
       if (on) {
-        double2 t[NB];
 #pragma unroll
         for (int r = 0; r < NB; ++r) {
           double2 acc = make_double2(0.0, 0.0);
 #pragma unroll
-          for (int j = 0; j < NB; ++j) acc = cfma(SA[r * LP + j], q[j], acc);
-          t[r] = acc;
+          for (int j = 0; j < NB; ++j) acc = cfma(SA[r * LP + j], SQ[j * LP + c], acc);
+          SV[r * LP + c] = acc;
         }
+      }
+      double2 m[NB];
+      if (on) {
 #pragma unroll
         for (int i = 0; i < NB; ++i) {
           double2 acc = make_double2(0.0, 0.0);
 #pragma unroll
-          for (int r = 0; r < NB; ++r) acc = cfma_cj(SQ[r * LP + i], t[r], acc);
+          for (int r = 0; r < NB; ++r) acc = cfma_cj(SQ[r * LP + i], SV[r * LP + c], acc);
           m[i] = acc;
         }
       }
