@@ -771,8 +771,9 @@ __device__ __forceinline__ void eig_cols(int nk, const double2* __restrict__ A, 
       }
     }
     if (rotate) {  // SA <- Q^H F Q, column c
-      // t = A q_c goes through this lane's column of SV (free until V is formed) and
-      // q_c through SQ, so that only one nb-vector is live in registers at a time
+      // q_c goes through SQ and t = A q_c through this lane's column of SV (free until V
+      // is formed), and Q^H t straight into the lane's column of SA: no nb-vector is held
+      // in registers across a barrier (at the 128-register cap of nb 5-8 they spilled)
       if (on) {
 #pragma unroll
         for (int r = 0; r < NB; ++r) SQ[r * LP + c] = Qin[base + (size_t)r * NB];
@@ -787,20 +788,15 @@ __device__ __forceinline__ void eig_cols(int nk, const double2* __restrict__ A, 
           SV[r * LP + c] = acc;
         }
       }
-      double2 m[NB];
+      __syncwarp();  // every lane has read A: its column can take (Q^H A q_c) entry by entry
       if (on) {
 #pragma unroll
         for (int i = 0; i < NB; ++i) {
           double2 acc = make_double2(0.0, 0.0);
 #pragma unroll
           for (int r = 0; r < NB; ++r) acc = cfma_cj(SQ[r * LP + i], SV[r * LP + c], acc);
-          m[i] = acc;
+          SA[i * LP + c] = acc;
         }
-      }
-      __syncwarp();
-      if (on) {
-#pragma unroll
-        for (int r = 0; r < NB; ++r) SA[r * LP + c] = m[r];
       }
     }
     __syncwarp();
