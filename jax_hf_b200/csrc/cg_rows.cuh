@@ -238,8 +238,9 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_rows_density(int nk, const d
 }
 
 // ----------------------------------- grad1: Ft, eps, G, g_p and four norms ---
+// 4 CTAs per SM: 128 registers without spills (16 warps per SM instead of 12)
 template <int NB>
-__global__ void __launch_bounds__(32 * kRowWarps) k_cgr_grad1(CgArgs a) {
+__global__ void __launch_bounds__(32 * kRowWarps, 4) k_cgr_grad1(CgArgs a) {
   if (!cg_active(a)) return;
   double2* const Qc = q_cur(a);
   using RG = RowGroup<NB>;
@@ -365,8 +366,11 @@ __device__ __forceinline__ double diag_uhfu_col(const double2 (&u)[NB], const do
 // would write if tau0 is accepted: eps = diag(U^H Ft U) into eps and Q U into Vd
 // (same arithmetic as k_cgr_update); its last CTA sets first_ok when tau0 is
 // accepted, and k_cgr_update then only copies Vd into Q.
+// the first trial (NT = 1) and the update at 3 CTAs per SM (at most 168 registers: 12
+// warps per SM instead of 8, with at most 24 B of spills at nb = 8); the backtracking
+// trials keep the registers they need
 template <int NB, int NT>
-__global__ void __launch_bounds__(32 * kRowWarps) k_cgr_trials(CgArgs a, int i0, int i1, int last_chunk) {
+__global__ void __launch_bounds__(32 * kRowWarps, NT == 1 ? 3 : 1) k_cgr_trials(CgArgs a, int i0, int i1, int last_chunk) {
   if (!cg_active(a)) return;
   if (a.sc->accepted) return;
   using RG = RowGroup<NB>;
@@ -474,7 +478,7 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_cgr_trials(CgArgs a, int i0,
 
 // ----------------- retraction: U(tau), Q <- Q U, eps_new = diag(U^H Ft U)
 template <int NB>
-__global__ void __launch_bounds__(32 * kRowWarps) k_cgr_update(CgArgs a) {
+__global__ void __launch_bounds__(32 * kRowWarps, 3) k_cgr_update(CgArgs a) {
   if (!cg_active(a)) return;
   if (a.sc->first_ok) return;  // tau0 accepted: the first trial formed eps and Q U(tau0) already
   double2* const Qc = q_cur(a);
