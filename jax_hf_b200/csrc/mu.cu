@@ -207,10 +207,16 @@ __device__ __forceinline__ double expit(double x) { return 1.0 / (1.0 + exp(-x))
 // Dev. 34 (1990) 111-119: with y the correctly rounded 1/b and q faithful, r = x - q b is
 // exact under an fma and q + r y rounds to the correctly rounded x / b) a second step
 // gives the correctly rounded quotient, the bits of x / b.  The remainder must not
-// underflow, so numerators below 2^-900 in magnitude (and NaN) take the division.
-// Five fp64 operations in place of a division routine per element, at the same bits.
+// underflow nor the products overflow, so numerators outside [2^-900, 2^900] in
+// magnitude (and NaN and infinities) take the division, and so does every x when
+// rb = 0 (recip_of: divisors outside [2^-64, 2^64]).  Five fp64 operations in place
+// of a division routine per element, at the same bits.
+__device__ __forceinline__ double recip_of(double b) {
+  return (fabs(b) >= 0x1p-64 && fabs(b) <= 0x1p+64) ? 1.0 / b : 0.0;
+}
 __device__ __forceinline__ double div_by(double x, double b, double rb) {
-  if (!(fabs(x) >= 0x1p-900)) return x / b;
+  const double ax = fabs(x);
+  if (!(ax >= 0x1p-900 && ax <= 0x1p+900) || rb == 0.0) return x / b;
   double q = x * rb;
   double r = fma(-q, b, x);
   q = fma(r, rb, q);
@@ -264,7 +270,7 @@ __global__ void __launch_bounds__(BT) k_find_mu(const MuArgs a) {
   // are the first Newton evaluation whenever mu0 lies inside the bracket.
   const bool fuse_first = NEWTON && a.method == 2 && a.mu0 != nullptr;
   const double mu0v = fuse_first ? a.mu0[0] : 0.0;
-  const double Tf = fmax(a.T, 1e-12), rTf = 1.0 / Tf;
+  const double Tf = fmax(a.T, 1e-12), rTf = recip_of(Tf);
   double mn = INFINITY, mx = -INFINITY, N0 = 0.0, Z0 = 0.0;
   if (fuse_first) {
     visit([&](double v, double w) {
@@ -427,7 +433,7 @@ __global__ void __launch_bounds__(BT) k_find_mu(const MuArgs a) {
     }
     result = 0.5 * (lo + hi);
   } else {
-    const double Tj = fmax(a.T, 1e-12), rTj = 1.0 / Tj;
+    const double Tj = fmax(a.T, 1e-12), rTj = recip_of(Tj);
     double lo, hi, mu;
     if (a.method == 1) {
       const double span = mx - mn + 10.0 * fmax(Tj, 1e-6);
